@@ -1,0 +1,386 @@
+"""Benchmark of the Fourier central-slice hot path on B200 (one JSON line on rank 0).
+
+Workload (one step = one pass of the hot path over one batch):
+  extract_central_slices_3d<"hc2h">   4096 slices of 256x129 complex64 from a 256^3 rfft volume (LINEAR, cutoff 0.5)
+  rasterize_central_slices_3d<"h2hc"> 4096 slices of 256x129 complex64 into a 256^3 rfft volume + f32 weights
+Synthetic, seeded inputs: volume amplitude 1/max(|f|,1/64), slices complex Gaussian x exp(-100 f^2/4),
+uniform SO(3) orientations. Metric: slices/s (extract + insert slices per second, whole job).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1 runs under torchrun, one rank per GPU: every rank processes its own 4096 + 4096 slices (weak
+scaling; extraction needs no exchange, and the insertion's partial grids are summed by one NCCL
+all-reduce after the timed region, as a reconstruction does once at its end).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N = 256
+SLICES = 4096
+BFACTOR = 100.0
+L2_FLUSH_BYTES = 256 << 20      # > 126 MB L2
+
+
+def algorithmic_bytes(n: int, b: int) -> dict:
+    """Compulsory bytes per launch (volume/slices read or written once; Mat33 read once per slice)."""
+    v = n * n * (n // 2 + 1)
+    p = n * (n // 2 + 1)
+    return {"extract": 8 * v + b * (8 * p + 48),
+            "rasterize": b * (8 * p + 48) + 2 * (8 * v + 4 * v)}
+
+
+def measured_peaks() -> dict:
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def profiled_traffic() -> dict:
+    """DRAM bytes per launch from the committed ncu summary (profiles/), if present."""
+    path = os.path.join(ROOT, "profiles", "extract_rasterize_256.md")
+    out = {}
+    if os.path.exists(path):
+        for line in open(path):
+            m = re.match(r"\s*traffic_bytes_per_launch\.(\w+)\s*[:=]\s*([0-9.eE+]+)", line)
+            if m:
+                out[m.group(1)] = float(m.group(2))
+    return out
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while the timed region runs."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in getattr(self, "lines", []):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def make_inputs(seed: int):
+    import torch
+    from noa_b200 import synthetic
+    from noa_b200.fourier_project import pack_rotations
+    dev = "cuda"
+    vol = torch.from_numpy(synthetic.make_volume(N, seed=seed)).to(dev)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed + 1)
+    shape = (SLICES, 1, N, N // 2 + 1)
+    re = torch.randn(shape, generator=g, device=dev)
+    im = torch.randn(shape, generator=g, device=dev)
+    env = torch.from_numpy(np.exp(-BFACTOR * synthetic.slice_fftfreq_norm((N, N), centered=False) ** 2 / 4)
+                           .astype(np.float32)).to(dev)
+    slices = (torch.complex(re, im) * (env / math.sqrt(2))).contiguous()
+    del re, im
+    rot_e = pack_rotations(torch.from_numpy(synthetic.random_rotations(SLICES, seed=seed + 2)).to(dev))
+    rot_i = pack_rotations(torch.from_numpy(synthetic.random_rotations(SLICES, seed=seed + 3)).to(dev))
+    return vol, slices, rot_e, rot_i
+
+
+def run_gpu(args) -> None:
+    import torch
+    import torch.distributed as dist
+    from noa_b200 import fourier_project as fp
+
+    world, rank, local = dist_setup()
+    vol, slices_in, rot_e, rot_i = make_inputs(seed=1000 * rank)
+    out = torch.empty((SLICES, 1, N, N // 2 + 1), dtype=torch.complex64, device="cuda")
+    grid = torch.zeros((1, N, N, N // 2 + 1), dtype=torch.complex64, device="cuda")
+    grid_w = torch.zeros((1, N, N, N // 2 + 1), dtype=torch.float32, device="cuda")
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+    vshape, sshape = (1, N, N, N), (SLICES, 1, N, N)
+
+    def extract():
+        fp.extract_central_slices_3d("hc2h", vol, None, vshape, out, None, sshape, None, rot_e,
+                                     fftfreq_cutoff=0.5, stream=stream)
+
+    def rasterize():
+        fp.rasterize_central_slices_3d("h2hc", slices_in, None, sshape, grid, grid_w, vshape, None, rot_i,
+                                       fftfreq_cutoff=0.5, stream=stream)
+
+    for _ in range(args.warmup):
+        extract()
+        rasterize()
+    torch.cuda.synchronize()
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        for k in range(args.steps):
+            flush.fill_(float(k))          # L2 flush between timed steps (outside the events)
+            e0, e1, e2 = ev[k]
+            e0.record(stream)
+            extract()
+            e1.record(stream)
+            rasterize()
+            e2.record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t_ext = [a.elapsed_time(b) for a, b, _ in ev]
+    t_ras = [b.elapsed_time(c) for _, b, c in ev]
+    step_ms = sum(t_ext + t_ras) / args.steps
+    ext_ms, ras_ms = statistics.mean(t_ext), statistics.mean(t_ras)
+    if world > 1:
+        t = torch.tensor([step_ms, ext_ms, ras_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        step_ms, ext_ms, ras_ms = t.tolist()
+        # The reconstruction's one exchange: sum the per-rank partial grids (after the timed region).
+        dist.all_reduce(grid)
+        dist.all_reduce(grid_w)
+        torch.cuda.synchronize()
+
+    # End to end through the public API with host buffers: H2D of the step's inputs (volume,
+    # slices to insert, rotations) from pinned memory, both calls, D2H of the results.
+    h_vol = vol.cpu().pin_memory()
+    h_slices = slices_in.cpu().pin_memory()
+    h_rot_e, h_rot_i = rot_e.cpu().pin_memory(), rot_i.cpu().pin_memory()
+    h_out = torch.empty(out.shape, dtype=out.dtype).pin_memory()
+    h_grid = torch.empty(grid.shape, dtype=grid.dtype).pin_memory()
+    h_grid_w = torch.empty(grid_w.shape, dtype=grid_w.dtype).pin_memory()
+    bi = (h_vol.numel() * 8 + h_slices.numel() * 8 + h_rot_e.numel() * 4 + h_rot_i.numel() * 4)
+    bo = h_out.numel() * 8 + h_grid.numel() * 8 + h_grid_w.numel() * 4
+    e2e_steps = max(2, min(args.e2e_steps, args.steps))
+    e2e_ms = []
+    for k in range(e2e_steps + 1):
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        vol.copy_(h_vol, non_blocking=True)
+        slices_in.copy_(h_slices, non_blocking=True)
+        rot_e.copy_(h_rot_e, non_blocking=True)
+        rot_i.copy_(h_rot_i, non_blocking=True)
+        extract()
+        rasterize()
+        h_out.copy_(out, non_blocking=True)
+        h_grid.copy_(grid, non_blocking=True)
+        h_grid_w.copy_(grid_w, non_blocking=True)
+        s1.record(stream)
+        torch.cuda.synchronize()
+        if k > 0:
+            e2e_ms.append(s0.elapsed_time(s1))
+    e2e = statistics.mean(e2e_ms)
+    if world > 1:
+        t = torch.tensor([e2e], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e = t.item()
+
+    if rank == 0:
+        ab = algorithmic_bytes(N, SLICES)
+        peaks = measured_peaks()
+        traffic = profiled_traffic()
+        dom = "rasterize" if ras_ms >= ext_ms else "extract"
+        dom_ms = ras_ms if dom == "rasterize" else ext_ms
+        achieved = ab[dom] / (dom_ms * 1e-3) / 1e9
+        total_slices = 2 * SLICES * world
+        line = {
+            "metric": "slices/sec extract & insert at 256^3",
+            "value": total_slices / (step_ms * 1e-3),
+            "unit": "slices/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": step_ms,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic (seeded; no dataset)",
+            "config": {"workload": "extract 4096 + rasterize 4096 slices of 256x129 c64, 256^3 rfft volume (+f32 weights)",
+                       "volume": [N, N, N // 2 + 1], "slices_per_op": SLICES, "remaps": ["hc2h", "h2hc"],
+                       "interp": "linear", "fftfreq_cutoff": 0.5, "l2": "flushed between timed steps (256 MB write)",
+                       "parallelism": f"slice shards x{world}"},
+            "per_op": {"extract_ms": ext_ms, "rasterize_ms": ras_ms,
+                       "extract_slices_per_s": SLICES * world / (ext_ms * 1e-3),
+                       "insert_slices_per_s": SLICES * world / (ras_ms * 1e-3),
+                       "extract_gbs": ab["extract"] / (ext_ms * 1e-3) / 1e9,
+                       "rasterize_gbs": ab["rasterize"] / (ras_ms * 1e-3) / 1e9},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peaks["hbm_gbs"],
+                         "peak_source": peaks["source"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+                         "algorithmic_bytes": ab[dom], "traffic": traffic.get(dom)},
+            "e2e": {"value": total_slices / (e2e * 1e-3), "unit": "slices/s", "h2d_bytes_per_step": bi,
+                    "d2h_bytes_per_step": bo, "ms_per_step": e2e},
+            "gpu_launches": 2 * args.steps,
+            "clocks": clocks.summary(),
+        }
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------------------------------
+# CPU: noa's own CPU path (oracle/_ref, built from the reference sources) or the C restatement.
+# ---------------------------------------------------------------------------------------------------
+def _cpu_sample(batch: int, seed: int = 7):
+    from noa_b200 import synthetic
+    from oracle.oracle import Call
+    vol = synthetic.make_volume(N, seed=seed)
+    slices = synthetic.make_slices(batch, N, seed=seed + 1, bfactor=BFACTOR)
+    rot_e = synthetic.random_rotations(batch, seed=seed + 2)
+    rot_i = synthetic.random_rotations(batch, seed=seed + 3)
+    ext = Call(func="extract", remap="hc2h", inp=vol, in_shape=(1, N, N, N),
+               out=np.zeros((batch, 1, N, N // 2 + 1), np.complex64), out_shape=(batch, 1, N, N), rot=rot_e)
+    ras = Call(func="rasterize", remap="h2hc", inp=slices, in_shape=(batch, 1, N, N),
+               out=np.zeros((1, N, N, N // 2 + 1), np.complex64), out_shape=(1, N, N, N), rot=rot_i,
+               out_w=np.zeros((1, N, N, N // 2 + 1), np.float32))
+    return ext, ras
+
+
+def _cpu_impl():
+    from oracle.oracle import FpOracle, RefLib, ref_available
+    if ref_available():
+        lib = RefLib()
+        return "reference", (lambda call, thr: lib.run(call, thr)[0])
+    lib = FpOracle()
+    return "port", (lambda call, thr: lib.run(call, thr))
+
+
+def cpu_baseline(seconds: float) -> dict:
+    """noa's CPU path timed on this host's cores over a bounded sample of the workload."""
+    kind, run = _cpu_impl()
+    threads = os.cpu_count() or 1
+    batch = 32
+    ext, ras = _cpu_sample(batch)
+    run(ext, threads)           # warm-up
+    run(ras, threads)
+    done, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        run(ext, threads)
+        run(ras, threads)
+        done += 2 * batch
+    dt = time.perf_counter() - t0
+    return {"value": done / dt, "unit": "slices/s", "cores": threads, "kind": kind,
+            "sample": f"{done} slices ({batch}-slice extract + {batch}-slice rasterize batches, 256^3, "
+                      f"{dt:.1f} s, threads={threads}; rasterize runs with noa's per-float omp atomics)"}
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    kind, run = _cpu_impl()
+    threads = os.cpu_count() or 1
+    batch = args.ref_batch
+    ext, ras = _cpu_sample(batch)
+    for _ in range(args.warmup):
+        run(ext, threads)
+        run(ras, threads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        run(ext, threads)
+        run(ras, threads)
+        times.append(time.perf_counter() - t0)
+    step = statistics.mean(times)
+    value = 2 * batch / step
+    print(json.dumps({
+        "impl": "reference",
+        "metric": "slices/sec extract & insert at 256^3",
+        "value": value, "unit": "slices/s", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": step * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded; no dataset)",
+        "config": {"workload": "extract + rasterize slices of 256x129 c64, 256^3 rfft volume (+f32 weights)",
+                   "slices_per_op_per_step": batch, "remaps": ["hc2h", "h2hc"], "interp": "linear"},
+        "cpu_baseline": {"value": value, "unit": "slices/s", "cores": threads, "kind": kind,
+                         "sample": f"{batch}-slice extract + {batch}-slice rasterize per step, {threads} threads"},
+        "e2e": {"value": value, "unit": "slices/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main() -> None:
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=400)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", choices=["noa_b200", "reference"], default="noa_b200")
+    p.add_argument("--e2e-steps", type=int, default=5)
+    p.add_argument("--cpu-seconds", type=float, default=12.0)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--ref-batch", type=int, default=32)
+    args = p.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

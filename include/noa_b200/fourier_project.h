@@ -1,0 +1,137 @@
+/* noa_b200 — B200-native (sm_100a) Fourier central-slice extraction and insertion.
+ *
+ * C ABI of the drop-in. Each entry point replaces the GPU branch of one noa function template in
+ * noa/xform/FourierProject.hpp (the `details::launch_*<REMAP, i32, true>` call inside
+ * `#ifdef NOA_ENABLE_GPU`), keeping its argument meaning, layouts and results:
+ *
+ *   nb_rasterize_central_slices_3d            <- rasterize_central_slices_3d            FourierProject.hpp:1653-1692 (GPU branch :1675-1685)
+ *   nb_insert_central_slices_3d               <- insert_central_slices_3d               FourierProject.hpp:1770-1815 (GPU branch :1792-1808)
+ *   nb_extract_central_slices_3d              <- extract_central_slices_3d              FourierProject.hpp:1869-1914 (GPU branch :1891-1907)
+ *   nb_insert_and_extract_central_slices_3d   <- insert_and_extract_central_slices_3d   FourierProject.hpp:1987-2049 (GPU branch :2022-2041)
+ *
+ * All array and transform pointers are DEVICE pointers on the current CUDA device. Calls are
+ * asynchronous on `stream` (a cudaStream_t; NULL = the legacy default stream). Return values are
+ * NB_OK or a negative NB_ERROR_*; nb_last_error() then describes the failure (thread-local). No kernel
+ * traps: invalid arguments are rejected on the host before any launch.
+ */
+#ifndef NOA_B200_FOURIER_PROJECT_H
+#define NOA_B200_FOURIER_PROJECT_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define NB_API __attribute__((visibility("default")))
+#else
+#define NB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    NB_OK = 0,
+    NB_ERROR_INVALID = -1,      /* bad argument (shape, stride, overlap, option): noa's check() failures */
+    NB_ERROR_UNSUPPORTED = -2,  /* valid for noa but not provided here (f64/c64 values, textures) */
+    NB_ERROR_CUDA = -3,         /* a CUDA runtime call failed */
+    NB_ERROR_OOM = -4,          /* a scratch or device allocation failed */
+    NB_ERROR_TIMEOUT = -5       /* a bounded device wait ran out (batched/serving paths only) */
+};
+
+/* noa::fft::Layout values of the four hx2hx remaps (fft/core/Layout.hpp:48-55). */
+enum { NB_REMAP_H2H = 0, NB_REMAP_H2HC = 8, NB_REMAP_HC2H = 4, NB_REMAP_HC2HC = 12 };
+
+/* noa::xform::Interp::Method values (xform/core/Interp.hpp:16-40). The _FAST variants (value + 100)
+ * only differ from the accurate ones for texture inputs, which this library does not take. */
+enum {
+    NB_INTERP_NEAREST = 0, NB_INTERP_LINEAR = 1, NB_INTERP_CUBIC = 2, NB_INTERP_CUBIC_BSPLINE = 3,
+    NB_INTERP_LANCZOS4 = 4, NB_INTERP_LANCZOS6 = 5, NB_INTERP_LANCZOS8 = 6
+};
+
+enum { NB_DTYPE_F32 = 1, NB_DTYPE_C32 = 2, NB_DTYPE_F64 = 3, NB_DTYPE_C64 = 4 };
+
+/* Transform kinds, in noa's memory layout: Mat22<f32> is 4 floats (16 bytes), Mat33<f32> is 9 floats
+ * row-major padded to 48 bytes (alignas 16), Quaternion<f32> is z,y,x,w (16 bytes). */
+enum { NB_XFORM_NONE = 0, NB_XFORM_MAT22_F32 = 1, NB_XFORM_MAT33_F32 = 2, NB_XFORM_QUAT_F32 = 3 };
+
+/* An array argument: noa's View/Array reduced to pointer, physical BDHW shape and element strides. */
+typedef struct {
+    void* data;             /* device pointer; NULL with is_value == 0 means "absent" (noa's Empty) */
+    int32_t dtype;          /* NB_DTYPE_* */
+    int32_t is_value;       /* 1: a single value (value[0] + i*value[1]) stands for every element */
+    int64_t shape[4];       /* physical shape, i.e. the logical shape's .rfft() */
+    int64_t strides[4];     /* strides in elements (any sign-free layout; 0 broadcasts) */
+    double value[2];
+} nb_array;
+
+/* A per-slice transform argument: a single value (data == NULL, count == 1) or a contiguous array. */
+typedef struct {
+    const void* data;       /* device pointer to `count` transforms, or NULL to use value[] */
+    int32_t kind;           /* NB_XFORM_*; NB_XFORM_NONE is only valid for scalings (noa's Empty) */
+    int64_t count;          /* 1 = the same transform for every slice, else the number of slices */
+    double value[9];        /* inline transform: Mat22 row-major (4), Mat33 row-major (9), quaternion z,y,x,w */
+} nb_transform;
+
+/* Union of noa's option structs (FourierProject.hpp:1602-1627, 1703-1739, 1817-1838, 1916-1951). */
+typedef struct {
+    int32_t interp;             /* NB_INTERP_* (+100 accepted); ignored by rasterize */
+    double fftfreq_cutoff;      /* default 0.5 */
+    int64_t target_shape[4];    /* BDHW; any zero element -> the grid shape (noa's default {}) */
+    double ews_radius[2];       /* HW Ewald sphere radius; {0,0} -> no curvature */
+    double fftfreq_sinc;        /* insert: windowed_sinc; insert_and_extract: input_windowed_sinc (default -1) */
+    double fftfreq_blackman;    /* (default -1) */
+    double w_fftfreq_sinc;      /* extract / insert_and_extract: w_windowed_sinc (default -1) */
+    double w_fftfreq_blackman;  /* (default -1) */
+    int32_t add_to_output;      /* insert_and_extract only */
+    int32_t correct_weights;    /* insert_and_extract only */
+} nb_options;
+
+/* Fills `o` with noa's defaults (LINEAR, cutoff 0.5, no target, no EWS, windowed-sinc {-1,-1}). */
+NB_API void nb_options_default(nb_options* o);
+
+/* rasterize_central_slices_3d: trilinear scatter of 2-D rfft slices into a 3-D rfft volume (+=).
+ * slice: B x 1 x H x W/2+1 (f32|c32, or a constant value); volume: 1 x D x H x W/2+1 (f32|c32);
+ * weights are f32 or absent. inv_scaling: Mat22 or NONE; fwd_rotation: Mat33 or quaternion. */
+NB_API int nb_rasterize_central_slices_3d(
+    int32_t remap,
+    const nb_array* slice, const nb_array* slice_weight, const int64_t slice_shape[4],
+    const nb_array* volume, const nb_array* volume_weight, const int64_t volume_shape[4],
+    const nb_transform* inv_scaling, const nb_transform* fwd_rotation,
+    const nb_options* options, void* stream);
+
+/* insert_central_slices_3d: windowed-sinc gather insertion, one output voxel at a time (+=).
+ * fwd_scaling: Mat22 or NONE; inv_rotation: Mat33 or quaternion. Deterministic. */
+NB_API int nb_insert_central_slices_3d(
+    int32_t remap,
+    const nb_array* slice, const nb_array* slice_weight, const int64_t slice_shape[4],
+    const nb_array* volume, const nb_array* volume_weight, const int64_t volume_shape[4],
+    const nb_transform* fwd_scaling, const nb_transform* inv_rotation,
+    const nb_options* options, void* stream);
+
+/* extract_central_slices_3d: 3-D spectrum interpolation at every pixel of every output slice (=). */
+NB_API int nb_extract_central_slices_3d(
+    int32_t remap,
+    const nb_array* volume, const nb_array* volume_weight, const int64_t volume_shape[4],
+    const nb_array* slice, const nb_array* slice_weight, const int64_t slice_shape[4],
+    const nb_transform* inv_scaling, const nb_transform* fwd_rotation,
+    const nb_options* options, void* stream);
+
+/* insert_and_extract_central_slices_3d: extraction from the virtual volume of the input slices. */
+NB_API int nb_insert_and_extract_central_slices_3d(
+    int32_t remap,
+    const nb_array* input_slice, const nb_array* input_weight, const int64_t input_slice_shape[4],
+    const nb_array* output_slice, const nb_array* output_weight, const int64_t output_slice_shape[4],
+    const nb_transform* input_fwd_scaling, const nb_transform* input_inv_rotation,
+    const nb_transform* output_inv_scaling, const nb_transform* output_fwd_rotation,
+    const nb_options* options, void* stream);
+
+/* Description of the last error on the calling thread ("" if none). */
+NB_API const char* nb_last_error(void);
+
+/* Library version, "major.minor.patch". */
+NB_API const char* nb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
