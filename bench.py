@@ -373,7 +373,11 @@ def main() -> None:
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--ref-batch", type=int, default=32)
+    p.add_argument("--n", type=int, default=256, help="box size (profiling runs use smaller cases)")
+    p.add_argument("--slices", type=int, default=4096, help="slices per op per step")
     args = p.parse_args()
+    global N, SLICES
+    N, SLICES = args.n, args.slices
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

@@ -205,6 +205,16 @@ Ews make_ews(const double r[2]) {
 
 float fmax_ref(float a, float b) { return a < b ? b : a; }
 
+// Whether an array's largest element offset needs more than 31 bits.
+bool needs_wide(const nb_array* a) {
+    if (!is_array(a))
+        return false;
+    int64_t extent = 0;
+    for (int i = 0; i < 4; ++i)
+        extent += (a->shape[i] - 1) * a->strides[i];
+    return extent >= (int64_t(1) << 31) - 1;
+}
+
 // blackman_window_size (FourierProject.hpp:114-137).
 int blackman_window_size(float fftfreq_blackman, float spectrum_size) {
     double samples = static_cast<double>(spectrum_size) * static_cast<double>(fftfreq_blackman);
@@ -454,6 +464,7 @@ int nb_extract_central_slices_3d(
     a.wsize = blackman_window_size(a.efb, t[0]);
     a.in_cplx = is_complex(volume->dtype);
     a.out_cplx = is_complex(slice->dtype);
+    a.wide_in = needs_wide(volume) || needs_wide(volume_weight);
     return finish(launch_extract(a, static_cast<cudaStream_t>(stream)));
 }
 

@@ -35,6 +35,7 @@ struct ProjArgs {
     int add_to_output, correct_weights;
 
     int in_cplx, out_cplx;     // value kinds (input/output complex?)
+    int wide_in;               // input offsets need 64 bits (an array spans >= 2^31 elements)
 };
 
 cudaError_t launch_extract(const ProjArgs& a, cudaStream_t stream);

@@ -381,6 +381,145 @@ __device__ __forceinline__ float2 interp_spectrum_2d(const SrcView& src, const S
     }
 }
 
+// ---------------------------------------------------------------------------------------------------
+// Lean 3-D reads: offsets in Idx (int32 when the array fits, else int64), no constant-value branch.
+// ---------------------------------------------------------------------------------------------------
+template<typename Idx>
+struct View3 {
+    const void* data;
+    Idx s0, s1, s2;
+};
+
+template<bool CPLX, typename Idx>
+__device__ __forceinline__ float2 view_read(const View3<Idx>& v, Idx off) {
+    if constexpr (CPLX)
+        return __ldg(static_cast<const float2*>(v.data) + off);
+    else
+        return make_float2(__ldg(static_cast<const float*>(v.data) + off), 0.f);
+}
+
+// interpolate_spectrum<LINEAR>, 3-D, rfft input (Interpolation.hpp:440-526): early Friedel flip, 2x2x2
+// taps with per-axis bounds and frequency2index done once per axis, sums in the reference's order.
+template<bool CPLX, typename Idx>
+__device__ __forceinline__ float2 interp_linear_3d(const View3<Idx>& v, const Spectrum3& sp,
+                                                   float q0, float q1, float q2) {
+    float conjugate = 1.f;
+    if (q2 < 0.f) {
+        q0 = -q0; q1 = -q1; q2 = -q2;
+        conjugate = -1.f;
+    }
+    const float fl0 = floorf(q0), fl1 = floorf(q1), fl2 = floorf(q2);
+    const int b0 = static_cast<int>(fl0), b1 = static_cast<int>(fl1), b2 = static_cast<int>(fl2);
+    const float t0 = sub(q0, fl0), t1 = sub(q1, fl1), t2 = sub(q2, fl2);
+    const float w0[2] = {sub(1.f, t0), t0};
+    const float w1[2] = {sub(1.f, t1), t1};
+    const float w2[2] = {sub(1.f, t2), t2};
+    const int lo0 = -sp.n0 / 2, hi0 = (sp.n0 - 1) / 2;
+    const int lo1 = -sp.n1 / 2, hi1 = (sp.n1 - 1) / 2;
+    const int hi2 = sp.n2 / 2;
+    bool ok0[2], ok1[2], ok2[2];
+    Idx o0[2], o1[2], o2[2];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const int z = b0 + k, y = b1 + k, x = b2 + k;
+        ok0[k] = z >= lo0 && z <= hi0;
+        ok1[k] = y >= lo1 && y <= hi1;
+        ok2[k] = x >= 0 && x <= hi2;
+        o0[k] = static_cast<Idx>(frequency2index(sp.centered, z, sp.n0)) * v.s0;
+        o1[k] = static_cast<Idx>(frequency2index(sp.centered, y, sp.n1)) * v.s1;
+        o2[k] = static_cast<Idx>(x) * v.s2;
+    }
+    float2 value = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int z = 0; z < 2; ++z) {
+        float2 vz = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int y = 0; y < 2; ++y) {
+            float2 vy = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int x = 0; x < 2; ++x) {
+                if (ok0[z] && ok1[y] && ok2[x])
+                    vy = cfma(view_read<CPLX>(v, o0[z] + o1[y] + o2[x]), w2[x], vy);
+            }
+            vz = cfma(vy, w1[y], vz);
+        }
+        value = cfma(vz, w0[z], value);
+    }
+    value.y *= conjugate;
+    return value;
+}
+
+// Generic interpolate_spectrum, 3-D, on a View3 (any window).
+template<int I, bool CPLX, typename Idx>
+__device__ __forceinline__ float2 interp_3d(const View3<Idx>& v, const Spectrum3& sp, float f0, float f1, float f2) {
+    if constexpr (I == I_LINEAR) {
+        return interp_linear_3d<CPLX>(v, sp, f0, f1, f2);
+    } else {
+        constexpr int SIZE = InterpTraits<I>::SIZE;
+        constexpr bool FLIP_EARLY = SIZE <= 2;
+        const int lo0 = -sp.n0 / 2, hi0 = (sp.n0 - 1) / 2;
+        const int lo1 = -sp.n1 / 2, hi1 = (sp.n1 - 1) / 2;
+        const int hi2 = sp.n2 / 2;
+        float conjugate = 1.f;
+        if (FLIP_EARLY && f2 < 0.f) {
+            f0 = -f0; f1 = -f1; f2 = -f2;
+            conjugate = -1.f;
+        }
+        if constexpr (I == I_NEAREST) {
+            // NEAREST returns before the early-flip conjugation (Interpolation.hpp:480-485).
+            const int i0 = static_cast<int>(roundf(f0));
+            const int i1 = static_cast<int>(roundf(f1));
+            const int i2 = static_cast<int>(roundf(f2));
+            float2 r = make_float2(0.f, 0.f);
+            if (i0 >= lo0 && i0 <= hi0 && i1 >= lo1 && i1 <= hi1 && i2 >= 0 && i2 <= hi2)
+                r = view_read<CPLX>(v, static_cast<Idx>(frequency2index(sp.centered, i0, sp.n0)) * v.s0 +
+                                       static_cast<Idx>(frequency2index(sp.centered, i1, sp.n1)) * v.s1 +
+                                       static_cast<Idx>(i2) * v.s2);
+            return r;
+        } else {
+            constexpr int START = -(SIZE - 1) / 2;
+            const float fl0 = floorf(f0), fl1 = floorf(f1), fl2 = floorf(f2);
+            const int b0 = static_cast<int>(fl0), b1 = static_cast<int>(fl1), b2 = static_cast<int>(fl2);
+            float w0[SIZE], w1[SIZE], w2[SIZE];
+            interp_weights<I>(sub(f0, fl0), w0);
+            interp_weights<I>(sub(f1, fl1), w1);
+            interp_weights<I>(sub(f2, fl2), w2);
+            float2 value = make_float2(0.f, 0.f);
+#pragma unroll (SIZE <= 4 ? SIZE : 1)
+            for (int z = 0; z < SIZE; ++z) {
+                float2 vz = make_float2(0.f, 0.f);
+#pragma unroll
+                for (int y = 0; y < SIZE; ++y) {
+                    float2 vy = make_float2(0.f, 0.f);
+#pragma unroll
+                    for (int x = 0; x < SIZE; ++x) {
+                        int t0 = b0 + START + z, t1 = b1 + START + y, t2 = b2 + START + x;
+                        float conj = 1.f;
+                        if (!FLIP_EARLY && t2 < 0) {
+                            t0 = -t0; t1 = -t1; t2 = -t2;
+                            conj = -1.f;
+                        }
+                        if (t0 >= lo0 && t0 <= hi0 && t1 >= lo1 && t1 <= hi1 && t2 >= 0 && t2 <= hi2) {
+                            float2 val = view_read<CPLX>(
+                                v, static_cast<Idx>(frequency2index(sp.centered, t0, sp.n0)) * v.s0 +
+                                   static_cast<Idx>(frequency2index(sp.centered, t1, sp.n1)) * v.s1 +
+                                   static_cast<Idx>(t2) * v.s2);
+                            if (!FLIP_EARLY)
+                                val.y *= conj;
+                            vy = cfma(val, w2[x], vy);
+                        }
+                    }
+                    vz = cfma(vy, w1[y], vz);
+                }
+                value = cfma(vz, w0[z], value);
+            }
+            if (FLIP_EARLY)
+                value.y *= conjugate;
+            return value;
+        }
+    }
+}
+
 // cast_or_abs_squared (base/Math.hpp:220-225): complex -> real stores |z|^2.
 template<bool IN_CPLX, bool OUT_CPLX>
 __device__ __forceinline__ float2 to_output(float2 v) {

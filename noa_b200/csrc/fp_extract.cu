@@ -1,51 +1,203 @@
 // extract_central_slices_3d on sm_100a: one thread per output pixel, 3-D spectrum interpolation of
 // the volume (FourierExtract, noa/xform/FourierProject.hpp:632-694).
 //
-// Work decomposition: a CTA owns 256 consecutive pixels of the flattened (y, u) plane of ONE slice,
-// so its rotation is uniform and its taps land on a compact patch of the volume, which the L1 and the
-// 126 MB L2 keep resident (a 256^3 complex64 rfft volume is 67.6 MB). Taps are read through the
-// non-coherent path (ld.global.nc); outputs are written once, coalesced.
+// Work decomposition: a CTA owns a 16x16 tile of one slice (blockIdx.x = tile, blockIdx.y strides
+// over slices), each warp a 4x8 sub-tile, so the rotation is uniform per CTA and a warp's taps fall on
+// a compact patch of the volume; the volume (67.6 MB at 256^3) stays resident in the 126 MB L2 and
+// taps are read through the non-coherent L1 path. Volume offsets are 32-bit whenever the volume fits,
+// and the LINEAR path resolves bounds and frequency2index once per axis rather than once per tap.
 //
 // The w-windowed form (wsize > 1) keeps the reference's semantics — outputs are the windowed sum over
 // the w offsets of the z-shifted samples — but sums in registers, in w order, instead of zeroing the
 // outputs and adding atomically, so it is deterministic and needs no extra pass.
 #include "fp_args.cuh"
+#include "fp_pool.cuh"
 
 namespace nb {
 namespace {
 
-constexpr int EXTRACT_THREADS = 256;
+constexpr int TY = 16, TX = 16, EXTRACT_THREADS = TY * TX;
 
-template<int I, bool IN_C, bool OUT_C>
+// ---------------------------------------------------------------------------------------------------
+// Fast LINEAR path over a pair copy of the volume.
+//
+// The copy is dense (D x H x W/2+1) and element (z, y, x) holds the two x-neighbours v[z][y][x] and
+// v[z][y][x+1] (zero past the last column) as one float4, so the 2x2x2 trilinear cell is 4 aligned
+// 16-byte loads instead of 8 scattered 8-byte ones. Each thread interpolates PAIR_PPT pixels (rows
+// y, y+16, ...) of one column, keeping more loads in flight. The taps, weights and summation order
+// are those of interp_linear_3d, so the results are bit-identical to the generic path.
+// ---------------------------------------------------------------------------------------------------
+constexpr int PAIR_PPT = 4;
+
+__global__ void make_pairs(const __grid_constant__ ProjArgs a, float4* __restrict__ pairs) {
+    const int D = a.vol_d, H = a.vol_h, WP = a.vol_w / 2 + 1;
+    const int64_t n = static_cast<int64_t>(D) * H * WP;
+    const float2* vol = static_cast<const float2*>(a.in.data);
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int x = static_cast<int>(i % WP);
+        const int64_t zy = i / WP;
+        const int y = static_cast<int>(zy % H), z = static_cast<int>(zy / H);
+        const int64_t off = z * a.in.s0 + y * a.in.s1 + x * a.in.s2;
+        const float2 v0 = vol[off];
+        const float2 v1 = x + 1 < WP ? vol[off + a.in.s2] : make_float2(0.f, 0.f);
+        pairs[i] = make_float4(v0.x, v0.y, v1.x, v1.y);
+    }
+}
+
+__device__ __forceinline__ float2 interp_linear_pairs(const float4* __restrict__ pairs, int sz, int sy,
+                                                      const Spectrum3& sp, float q0, float q1, float q2) {
+    float conjugate = 1.f;
+    if (q2 < 0.f) {
+        q0 = -q0; q1 = -q1; q2 = -q2;
+        conjugate = -1.f;
+    }
+    const float fl0 = floorf(q0), fl1 = floorf(q1), fl2 = floorf(q2);
+    const int b0 = static_cast<int>(fl0), b1 = static_cast<int>(fl1), b2 = static_cast<int>(fl2);
+    const float t0 = sub(q0, fl0), t1 = sub(q1, fl1), t2 = sub(q2, fl2);
+    const float w0[2] = {sub(1.f, t0), t0};
+    const float w1[2] = {sub(1.f, t1), t1};
+    const float w20 = sub(1.f, t2);
+    const int lo0 = -sp.n0 / 2, hi0 = (sp.n0 - 1) / 2;
+    const int lo1 = -sp.n1 / 2, hi1 = (sp.n1 - 1) / 2;
+    const int hi2 = sp.n2 / 2;
+    const bool okx0 = b2 >= 0 && b2 <= hi2;
+    const bool okx1 = b2 + 1 >= 0 && b2 + 1 <= hi2;
+    float2 value = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int z = 0; z < 2; ++z) {
+        const int iz = b0 + z;
+        const bool okz = iz >= lo0 && iz <= hi0;
+        const int oz = frequency2index(sp.centered, iz, sp.n0) * sz;
+        float2 vz = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int y = 0; y < 2; ++y) {
+            const int iy = b1 + y;
+            const bool oky = iy >= lo1 && iy <= hi1;
+            float2 vy = make_float2(0.f, 0.f);
+            if (okz && oky && okx0) {
+                const float4 p = __ldg(pairs + (oz + frequency2index(sp.centered, iy, sp.n1) * sy + b2));
+                vy = cfma(make_float2(p.x, p.y), w20, vy);
+                if (okx1)
+                    vy = cfma(make_float2(p.z, p.w), t2, vy);
+            }
+            vz = cfma(vy, w1[y], vz);
+        }
+        value = cfma(vz, w0[z], value);
+    }
+    value.y *= conjugate;
+    return value;
+}
+
+template<bool OUT_C>
 __global__ void __launch_bounds__(EXTRACT_THREADS)
-extract_kernel(const __grid_constant__ ProjArgs a, int tiles_per_slice, int64_t n_tiles) {
+extract_pairs_kernel(const __grid_constant__ ProjArgs a, const float4* __restrict__ pairs, int ntx) {
     const int wp = a.slice_w / 2 + 1;
-    const int plane = a.slice_h * wp;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int y0 = (blockIdx.x / ntx) * (TY * PAIR_PPT) + (warp >> 1) * 4 + (lane >> 3);
+    const int u = (blockIdx.x % ntx) * TX + (warp & 1) * 8 + (lane & 7);
+    if (u >= wp)
+        return;
     const Spectrum3 sp{a.vol_d, a.vol_h, a.vol_w, a.in_centered};
+    const int WP = a.vol_w / 2 + 1;
+    const int sz = a.vol_h * WP, sy = WP;
+    const bool has_out_w = a.out_w.present;
+    const float f1 = div(static_cast<float>(u), a.f_slice1);
+    float f0[PAIR_PPT];
+#pragma unroll
+    for (int r = 0; r < PAIR_PPT; ++r)
+        f0[r] = div(static_cast<float>(index2frequency(a.out_centered, y0 + r * TY, a.slice_h)), a.f_slice0);
+
+    for (int64_t b = blockIdx.y; b < a.n_slices; b += gridDim.y) {
+        float2 value[PAIR_PPT];
+        bool inside[PAIR_PPT];
+#pragma unroll
+        for (int r = 0; r < PAIR_PPT; ++r) {
+            float fz, fy, fx;
+            slice2grid(f0[r], f1, a.scale, a.rot, b, a.ews, fz, fy, fx);
+            value[r] = make_float2(0.f, 0.f);
+            inside[r] = y0 + r * TY < a.slice_h && dot3(fz, fy, fx, fz, fy, fx) <= a.cutoff_sqd;
+            if (inside[r])
+                value[r] = to_output<true, OUT_C>(interp_linear_pairs(
+                    pairs, sz, sy, sp, mul(fz, a.target0), mul(fy, a.target1), mul(fx, a.target2)));
+        }
+#pragma unroll
+        for (int r = 0; r < PAIR_PPT; ++r) {
+            const int y = y0 + r * TY;
+            if (y >= a.slice_h)
+                continue;
+            dst_store<OUT_C>(a.out, b, y, u, value[r]);
+            if (has_out_w)
+                store_real(a.out_w, b, y, u, inside[r] ? 1.f : 0.f);
+        }
+    }
+}
+
+// Whether the pair path applies: LINEAR, complex volume, no input weights, no EWS, no scaling, no
+// w-window, a dense copy addressable in 32 bits, and enough pixels to amortise the copy.
+bool use_pairs(const ProjArgs& a) {
+    const int64_t wp_vol = a.vol_w / 2 + 1;
+    const int64_t vox = static_cast<int64_t>(a.vol_d) * a.vol_h * wp_vol;
+    const int64_t pix = a.n_slices * a.slice_h * static_cast<int64_t>(a.slice_w / 2 + 1);
+    return a.interp == I_LINEAR && a.in_cplx && !a.in_w.present && !a.in.is_value && !a.ews.on &&
+           a.scale.kind == 0 && a.wsize <= 1 && vox < (int64_t(1) << 31) && pix >= 2 * vox;
+}
+
+cudaError_t launch_pairs(const ProjArgs& a, cudaStream_t stream, bool& done) {
+    done = false;
+    const int64_t wp_vol = a.vol_w / 2 + 1;
+    const int64_t vox = static_cast<int64_t>(a.vol_d) * a.vol_h * wp_vol;
+    float4* pairs = static_cast<float4*>(scratch_alloc(static_cast<size_t>(vox) * sizeof(float4), stream));
+    if (!pairs)
+        return cudaSuccess; // no scratch: the caller takes the generic path
+    const int threads = 256;
+    const int64_t blocks = (vox + threads - 1) / threads;
+    const int grid_c = static_cast<int>(blocks < static_cast<int64_t>(sm_count()) * 16 ? blocks : sm_count() * 16);
+    make_pairs<<<grid_c, threads, 0, stream>>>(a, pairs);
+    const int wp = a.slice_w / 2 + 1;
+    const int ntx = (wp + TX - 1) / TX, nty = (a.slice_h + TY * PAIR_PPT - 1) / (TY * PAIR_PPT);
+    const dim3 grid(static_cast<unsigned>(ntx * nty), static_cast<unsigned>(a.n_slices < 65535 ? a.n_slices : 65535));
+    if (a.out_cplx)
+        extract_pairs_kernel<true><<<grid, EXTRACT_THREADS, 0, stream>>>(a, pairs, ntx);
+    else
+        extract_pairs_kernel<false><<<grid, EXTRACT_THREADS, 0, stream>>>(a, pairs, ntx);
+    const cudaError_t err = cudaGetLastError();
+    scratch_free(pairs, stream);
+    done = err == cudaSuccess;
+    return err;
+}
+
+template<int I, bool IN_C, bool OUT_C, typename Idx>
+__global__ void __launch_bounds__(EXTRACT_THREADS)
+extract_kernel(const __grid_constant__ ProjArgs a, int ntx) {
+    const int wp = a.slice_w / 2 + 1;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int y = (blockIdx.x / ntx) * TY + (warp >> 1) * 4 + (lane >> 3);
+    const int u = (blockIdx.x % ntx) * TX + (warp & 1) * 8 + (lane & 7);
+    if (u >= wp || y >= a.slice_h)
+        return;
+    const Spectrum3 sp{a.vol_d, a.vol_h, a.vol_w, a.in_centered};
+    const View3<Idx> vol{a.in.data, static_cast<Idx>(a.in.s0), static_cast<Idx>(a.in.s1), static_cast<Idx>(a.in.s2)};
+    const View3<Idx> volw{a.in_w.data, static_cast<Idx>(a.in_w.s0), static_cast<Idx>(a.in_w.s1),
+                          static_cast<Idx>(a.in_w.s2)};
     const bool has_out_w = a.out_w.present;
     const bool has_in_w = a.in_w.present;
+    const int v = index2frequency(a.out_centered, y, a.slice_h);
+    const float f0 = div(static_cast<float>(v), a.f_slice0);
+    const float f1 = div(static_cast<float>(u), a.f_slice1);
 
-    for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
-        const int64_t b = tile / tiles_per_slice;
-        const int p = static_cast<int>(tile - b * tiles_per_slice) * EXTRACT_THREADS + static_cast<int>(threadIdx.x);
-        if (p >= plane)
-            continue;
-        const int y = p / wp;
-        const int u = p - y * wp;
-        const int v = index2frequency(a.out_centered, y, a.slice_h);
-
+    for (int64_t b = blockIdx.y; b < a.n_slices; b += gridDim.y) {
         float fz, fy, fx;
-        slice2grid(div(static_cast<float>(v), a.f_slice0), div(static_cast<float>(u), a.f_slice1),
-                   a.scale, a.rot, b, a.ews, fz, fy, fx);
+        slice2grid(f0, f1, a.scale, a.rot, b, a.ews, fz, fy, fx);
 
         float2 value = make_float2(0.f, 0.f);
         float weight = 0.f;
         if (a.wsize <= 1) {
             if (dot3(fz, fy, fx, fz, fy, fx) <= a.cutoff_sqd) {
                 const float q0 = mul(fz, a.target0), q1 = mul(fy, a.target1), q2 = mul(fx, a.target2);
-                value = to_output<IN_C, OUT_C>(interp_spectrum_3d<I, IN_C>(a.in, sp, q0, q1, q2));
+                value = to_output<IN_C, OUT_C>(interp_3d<I, IN_C>(vol, sp, q0, q1, q2));
                 if (has_out_w)
-                    weight = has_in_w ? interp_spectrum_3d<I, false>(a.in_w, sp, q0, q1, q2).x : 1.f;
+                    weight = has_in_w ? interp_3d<I, false>(volw, sp, q0, q1, q2).x : 1.f;
             }
         } else {
             for (int w = 0; w < a.wsize; ++w) {
@@ -55,10 +207,10 @@ extract_kernel(const __grid_constant__ ProjArgs a, int tiles_per_slice, int64_t 
                     continue;
                 const float q0 = mul(gz, a.target0), q1 = mul(fy, a.target1), q2 = mul(fx, a.target2);
                 const float cw = windowed_sinc(off, a.efs, a.efb);
-                const float2 iv = to_output<IN_C, OUT_C>(interp_spectrum_3d<I, IN_C>(a.in, sp, q0, q1, q2));
+                const float2 iv = to_output<IN_C, OUT_C>(interp_3d<I, IN_C>(vol, sp, q0, q1, q2));
                 value = cadd(value, cmul(iv, cw));
                 if (has_out_w) {
-                    const float iw = has_in_w ? interp_spectrum_3d<I, false>(a.in_w, sp, q0, q1, q2).x : 1.f;
+                    const float iw = has_in_w ? interp_3d<I, false>(volw, sp, q0, q1, q2).x : 1.f;
                     weight = add(weight, mul(iw, cw));
                 }
             }
@@ -72,14 +224,14 @@ extract_kernel(const __grid_constant__ ProjArgs a, int tiles_per_slice, int64_t 
 template<int I, bool IN_C, bool OUT_C>
 cudaError_t launch_typed(const ProjArgs& a, cudaStream_t stream) {
     const int wp = a.slice_w / 2 + 1;
-    const int plane = a.slice_h * wp;
-    const int tiles_per_slice = (plane + EXTRACT_THREADS - 1) / EXTRACT_THREADS;
-    const int64_t n_tiles = static_cast<int64_t>(tiles_per_slice) * a.n_slices;
-    if (n_tiles == 0)
+    const int ntx = (wp + TX - 1) / TX, nty = (a.slice_h + TY - 1) / TY;
+    if (a.n_slices == 0)
         return cudaSuccess;
-    const int64_t max_grid = static_cast<int64_t>(sm_count()) * 8 * 64;
-    const int grid = static_cast<int>(n_tiles < max_grid ? n_tiles : max_grid);
-    extract_kernel<I, IN_C, OUT_C><<<grid, EXTRACT_THREADS, 0, stream>>>(a, tiles_per_slice, n_tiles);
+    const dim3 grid(static_cast<unsigned>(ntx * nty), static_cast<unsigned>(a.n_slices < 65535 ? a.n_slices : 65535));
+    if (a.wide_in)
+        extract_kernel<I, IN_C, OUT_C, int64_t><<<grid, EXTRACT_THREADS, 0, stream>>>(a, ntx);
+    else
+        extract_kernel<I, IN_C, OUT_C, int32_t><<<grid, EXTRACT_THREADS, 0, stream>>>(a, ntx);
     return cudaGetLastError();
 }
 
@@ -95,6 +247,12 @@ cudaError_t launch_interp(const ProjArgs& a, cudaStream_t stream) {
 } // namespace
 
 cudaError_t launch_extract(const ProjArgs& a, cudaStream_t stream) {
+    if (a.n_slices > 0 && use_pairs(a)) {
+        bool done = false;
+        const cudaError_t err = launch_pairs(a, stream, done);
+        if (err != cudaSuccess || done)
+            return err;
+    }
     switch (a.interp) {
         case I_NEAREST: return launch_interp<I_NEAREST>(a, stream);
         case I_LINEAR: return launch_interp<I_LINEAR>(a, stream);

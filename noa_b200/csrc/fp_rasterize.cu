@@ -2,55 +2,77 @@
 // into the 2x2x2 voxels around its rotated frequency, plus the Hermitian-plane mirror taps
 // (FourierInsertRasterize, noa/xform/FourierProject.hpp:238-373).
 //
-// Complex values are added with one vector reduction (red.global.add.v2.f32, sm_90+) per tap instead
-// of two scalar ones; weights with a scalar f32 reduction.
+// The scatter is bound by the L2 reduction rate, which counts one operation per lane whatever its
+// width. So with output weights, a pixel's value and weight for one voxel travel in ONE reduction:
+// the kernel accumulates into a dense interleaved scratch grid — float4 (re, im, w, -) for complex
+// values, float2 (v, w) for real ones — taken from a stream-ordered pool, zeroed first, and a finalize
+// pass adds it into the caller's value and weight grids (whatever their strides). Without weights the
+// reductions go straight into the caller's grid (red.global.add.v2.f32 for complex values). If the
+// scratch cannot be allocated, the kernel falls back to two reductions per tap on the caller's grids.
+// CTAs own 16x16 pixel tiles of one slice (warps: 4x8), so a warp's reductions hit a compact patch.
 //
 // Deliberate deviation from the reference: the reference bounds the u tap by the LOGICAL volume width
 // (FourierProject.hpp:327-329), so a tap at u = W/2+1 passes and lands in the next row (or past the
 // end of the array). Here u is bounded by the physical width W/2+1. For even sizes and cutoffs <= 0.5
 // such taps carry a zero weight, so the results are the same.
 #include "fp_args.cuh"
+#include "fp_pool.cuh"
 
 namespace nb {
 namespace {
 
-constexpr int RASTER_THREADS = 256;
+constexpr int TY = 16, TX = 16, RASTER_THREADS = TY * TX;
 
-template<bool OUT_C>
-__device__ __forceinline__ void red_value(const DstView& d, int64_t iw, int64_t iv, int64_t iu, float2 v) {
-    const int64_t off = iw * d.s0 + iv * d.s1 + iu * d.s2;
-    if constexpr (OUT_C)
-        atomicAdd(static_cast<float2*>(d.data) + off, v);
-    else
-        atomicAdd(static_cast<float*>(d.data) + off, v.x);
-}
+enum Mode { DIRECT = 0, SCRATCH = 1 };
 
-__device__ __forceinline__ void red_weight(const DstView& d, int64_t iw, int64_t iv, int64_t iu, float w) {
-    atomicAdd(static_cast<float*>(d.data) + (iw * d.s0 + iv * d.s1 + iu * d.s2), w);
-}
+// Where one tap goes: the caller's grids (DIRECT) or the dense interleaved scratch (SCRATCH).
+template<bool OUT_C, int MODE>
+struct Sink {
+    DstView vol, volw;
+    void* scratch;
+    int sz, sy;           // dense scratch strides (x stride 1)
+    bool has_w;
 
-template<bool IN_C, bool OUT_C>
+    __device__ __forceinline__ void add(int iw, int iv, int iu, float2 v, float w) const {
+        if constexpr (MODE == SCRATCH) {
+            const int off = iw * sz + iv * sy + iu;
+            if constexpr (OUT_C)
+                atomicAdd(static_cast<float4*>(scratch) + off, make_float4(v.x, v.y, w, 0.f));
+            else
+                atomicAdd(static_cast<float2*>(scratch) + off, make_float2(v.x, w));
+        } else {
+            const int64_t off = iw * vol.s0 + iv * vol.s1 + iu * vol.s2;
+            if constexpr (OUT_C)
+                atomicAdd(static_cast<float2*>(vol.data) + off, v);
+            else
+                atomicAdd(static_cast<float*>(vol.data) + off, v.x);
+            if (has_w)
+                atomicAdd(static_cast<float*>(volw.data) + (iw * volw.s0 + iv * volw.s1 + iu * volw.s2), w);
+        }
+    }
+};
+
+template<bool IN_C, bool OUT_C, int MODE>
 __global__ void __launch_bounds__(RASTER_THREADS)
-rasterize_kernel(const __grid_constant__ ProjArgs a, int tiles_per_slice, int64_t n_tiles) {
+rasterize_kernel(const __grid_constant__ ProjArgs a, int ntx, void* scratch) {
     const int wp = a.slice_w / 2 + 1;
-    const int plane = a.slice_h * wp;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int y = (blockIdx.x / ntx) * TY + (warp >> 1) * 4 + (lane >> 3);
+    const int u = (blockIdx.x % ntx) * TX + (warp & 1) * 8 + (lane & 7);
+    if (u >= wp || y >= a.slice_h)
+        return;
     const int D = a.vol_d, H = a.vol_h, WP = a.vol_w / 2 + 1;
-    const bool vol_centered = a.out_centered;
+    const bool vc = a.out_centered;
     const bool has_out_w = a.out_w.present;
     const bool has_in_w = a.in_w.present;
+    const Sink<OUT_C, MODE> sink{a.out, a.out_w, scratch, H * WP, WP, has_out_w};
+    const int v = index2frequency(a.in_centered, y, a.slice_h);
+    const float f0 = div(static_cast<float>(v), a.f_slice0);
+    const float f1 = div(static_cast<float>(u), a.f_slice1);
 
-    for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
-        const int64_t b = tile / tiles_per_slice;
-        const int p = static_cast<int>(tile - b * tiles_per_slice) * RASTER_THREADS + static_cast<int>(threadIdx.x);
-        if (p >= plane)
-            continue;
-        const int y = p / wp;
-        const int u = p - y * wp;
-        const int v = index2frequency(a.in_centered, y, a.slice_h);
-
+    for (int64_t b = blockIdx.y; b < a.n_slices; b += gridDim.y) {
         float fz, fy, fx;
-        slice2grid(div(static_cast<float>(v), a.f_slice0), div(static_cast<float>(u), a.f_slice1),
-                   a.scale, a.rot, b, a.ews, fz, fy, fx);
+        slice2grid(f0, f1, a.scale, a.rot, b, a.ews, fz, fy, fx);
         if (dot3(fz, fy, fx, fz, fy, fx) > a.cutoff_sqd)
             continue;
 
@@ -83,12 +105,12 @@ rasterize_kernel(const __grid_constant__ ProjArgs a, int tiles_per_slice, int64_
 
 #pragma unroll
         for (int w = 0; w < 2; ++w) {
-            const int iw = frequency2index(vol_centered, b0 + w, D);
+            const int iw = frequency2index(vc, b0 + w, D);
             if (iw < 0 || iw >= D)
                 continue;
 #pragma unroll
             for (int vv = 0; vv < 2; ++vv) {
-                const int iv = frequency2index(vol_centered, b1 + vv, H);
+                const int iv = frequency2index(vc, b1 + vv, H);
                 if (iv < 0 || iv >= H)
                     continue;
                 const float kwv = mul(fr[w][0], fr[vv][1]);
@@ -98,9 +120,7 @@ rasterize_kernel(const __grid_constant__ ProjArgs a, int tiles_per_slice, int64_
                     if (iu < 0 || iu >= WP)
                         continue;
                     const float k = mul(kwv, fr[uu][2]);
-                    red_value<OUT_C>(a.out, iw, iv, iu, cmul(value, k));
-                    if (has_out_w)
-                        red_weight(a.out_w, iw, iv, iu, mul(weight, k));
+                    sink.add(iw, iv, iu, cmul(value, k), mul(weight, k));
                 }
             }
         }
@@ -112,35 +132,75 @@ rasterize_kernel(const __grid_constant__ ProjArgs a, int tiles_per_slice, int64_
                 cv.y = -cv.y;
 #pragma unroll
             for (int w = 0; w < 2; ++w) {
-                const int iw = frequency2index(vol_centered, -(b0 + w), D);
+                const int iw = frequency2index(vc, -(b0 + w), D);
                 if (iw < 0 || iw >= D)
                     continue;
 #pragma unroll
                 for (int vv = 0; vv < 2; ++vv) {
-                    const int iv = frequency2index(vol_centered, -(b1 + vv), H);
+                    const int iv = frequency2index(vc, -(b1 + vv), H);
                     if (iv < 0 || iv >= H)
                         continue;
                     const float k = mul(mul(fr[w][0], fr[vv][1]), fr[0][2]);
-                    red_value<OUT_C>(a.out, iw, iv, 0, cmul(cv, k));
-                    if (has_out_w)
-                        red_weight(a.out_w, iw, iv, 0, mul(weight, k));
+                    sink.add(iw, iv, 0, cmul(cv, k), mul(weight, k));
                 }
             }
         }
     }
 }
 
+// grid += scratch values; weights += scratch weights (caller's strides).
+template<bool OUT_C>
+__global__ void finalize_kernel(const __grid_constant__ ProjArgs a, const void* __restrict__ scratch) {
+    const int D = a.vol_d, H = a.vol_h, WP = a.vol_w / 2 + 1;
+    const int64_t n = static_cast<int64_t>(D) * H * WP;
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int x = static_cast<int>(i % WP);
+        const int64_t zy = i / WP;
+        const int y = static_cast<int>(zy % H), z = static_cast<int>(zy / H);
+        float2 v;
+        float w;
+        if constexpr (OUT_C) {
+            const float4 s = static_cast<const float4*>(scratch)[i];
+            v = make_float2(s.x, s.y);
+            w = s.z;
+        } else {
+            const float2 s = static_cast<const float2*>(scratch)[i];
+            v = make_float2(s.x, 0.f);
+            w = s.y;
+        }
+        dst_store<OUT_C>(a.out, z, y, x, cadd(dst_load<OUT_C>(a.out, z, y, x), v));
+        store_real(a.out_w, z, y, x, add(load_real(a.out_w, z, y, x), w));
+    }
+}
+
 template<bool IN_C, bool OUT_C>
 cudaError_t launch_typed(const ProjArgs& a, cudaStream_t stream) {
     const int wp = a.slice_w / 2 + 1;
-    const int plane = a.slice_h * wp;
-    const int tiles_per_slice = (plane + RASTER_THREADS - 1) / RASTER_THREADS;
-    const int64_t n_tiles = static_cast<int64_t>(tiles_per_slice) * a.n_slices;
-    if (n_tiles == 0)
+    const int ntx = (wp + TX - 1) / TX, nty = (a.slice_h + TY - 1) / TY;
+    if (a.n_slices == 0)
         return cudaSuccess;
-    const int64_t max_grid = static_cast<int64_t>(sm_count()) * 8 * 64;
-    const int grid = static_cast<int>(n_tiles < max_grid ? n_tiles : max_grid);
-    rasterize_kernel<IN_C, OUT_C><<<grid, RASTER_THREADS, 0, stream>>>(a, tiles_per_slice, n_tiles);
+    const dim3 grid(static_cast<unsigned>(ntx * nty), static_cast<unsigned>(a.n_slices < 65535 ? a.n_slices : 65535));
+    const int64_t vox = static_cast<int64_t>(a.vol_d) * a.vol_h * (a.vol_w / 2 + 1);
+    void* scratch = nullptr;
+    if (a.out_w.present && vox < (int64_t(1) << 31)) {
+        const size_t bytes = static_cast<size_t>(vox) * (OUT_C ? sizeof(float4) : sizeof(float2));
+        scratch = scratch_alloc(bytes, stream);
+        if (scratch && cudaMemsetAsync(scratch, 0, bytes, stream) != cudaSuccess) {
+            scratch_free(scratch, stream);
+            return cudaGetLastError();
+        }
+    }
+    if (scratch) {
+        rasterize_kernel<IN_C, OUT_C, SCRATCH><<<grid, RASTER_THREADS, 0, stream>>>(a, ntx, scratch);
+        const int64_t blocks = (vox + 255) / 256;
+        const int grid_f = static_cast<int>(blocks < static_cast<int64_t>(sm_count()) * 16 ? blocks : sm_count() * 16);
+        finalize_kernel<OUT_C><<<grid_f, 256, 0, stream>>>(a, scratch);
+        const cudaError_t err = cudaGetLastError();
+        scratch_free(scratch, stream);
+        return err;
+    }
+    rasterize_kernel<IN_C, OUT_C, DIRECT><<<grid, RASTER_THREADS, 0, stream>>>(a, ntx, nullptr);
     return cudaGetLastError();
 }
 

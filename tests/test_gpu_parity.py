@@ -114,3 +114,47 @@ def test_gpu_constant_input_rasterize():
     out, out_w = gpu_run.run(clone(call))
     assert rel_l2(out, ref.out) <= 1e-4
     assert rel_l2(out_w, ref.out_w) <= 1e-4
+
+
+@pytest.mark.parametrize("remap", ["h2h", "h2hc", "hc2h", "hc2hc"])
+@pytest.mark.parametrize("out_dt", ["c32", "f32"])
+def test_gpu_extract_pair_path(remap, out_dt):
+    """Enough slices that extraction takes the pair-copy fast path (pixels >= 2 x voxels)."""
+    import gpu_run
+    call = build(default_case("extract", remap=remap, n=32, nslices=80, out_dt=out_dt, out_w=True, seed=640))
+    ref = clone(call)
+    FpOracle().run(ref, 8)
+    out, out_w = gpu_run.run(clone(call))
+    assert rel_l2(out, ref.out) <= 1e-5
+    assert rel_l2(out_w, ref.out_w) <= 1e-5
+
+
+def test_gpu_extract_pair_path_bit_identical_to_generic():
+    """The pair path and the generic path (forced by an identity scaling) give identical bits."""
+    import torch
+    import gpu_run
+    call = build(default_case("extract", remap="hc2h", n=48, nslices=96, seed=641))
+    a, _ = gpu_run.run(clone(call))
+    call.scale = np.repeat(np.eye(2, dtype=np.float32)[None], 96, axis=0)
+    b, _ = gpu_run.run(clone(call))
+    np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("out_w", [False, True])
+@pytest.mark.parametrize("dts", [("c32", "c32"), ("c32", "f32"), ("f32", "f32")])
+def test_gpu_rasterize_accumulator_paths(out_w, dts):
+    """Rasterization through the interleaved scratch (weights) and straight into the grid (no weights),
+    accumulating on top of existing grid contents."""
+    import gpu_run
+    call = build(default_case("rasterize", remap="h2hc", n=48, nslices=40, in_dt=dts[0], out_dt=dts[1],
+                              out_w=out_w, in_w=out_w, seed=650))
+    rng = np.random.default_rng(5)
+    call.out[...] = rng.standard_normal(call.out.shape).astype(call.out.dtype)
+    if out_w:
+        call.out_w[...] = rng.uniform(0, 1, call.out_w.shape).astype(np.float32)
+    ref = clone(call)
+    FpOracle().run(ref, 1)
+    out, ow = gpu_run.run(clone(call))
+    assert rel_l2(out, ref.out) <= 1e-4
+    if out_w:
+        assert rel_l2(ow, ref.out_w) <= 1e-4
