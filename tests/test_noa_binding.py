@@ -1,0 +1,21 @@
+"""CPU test: the reference-side binding (include/noa_b200/noa_binding.hpp) compiles against noa's own
+headers for every function and argument kind. Needs the reference sources; skipped where absent."""
+import os
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF = "/root/reference/src"
+
+
+@pytest.mark.skipif(not os.path.isdir(os.path.join(REF, "noa")), reason="reference sources not present")
+def test_binding_compiles_against_noa_headers():
+    import torch
+    torch_inc = os.path.join(os.path.dirname(torch.__file__), "include")
+    cmd = ["g++", "-std=c++20", "-fsyntax-only", "-DNOA_ERROR_POLICY=2", "-DNOA_ENABLE_CPU", "-DFMT_HEADER_ONLY",
+           "-I", REF, "-I", os.path.join(ROOT, "include"), "-isystem", torch_inc,
+           "-isystem", os.path.join(ROOT, "oracle", "ref_shim"),
+           os.path.join(ROOT, "tests", "cpp", "noa_binding_compile.cpp")]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-4000:]
