@@ -125,6 +125,22 @@ NB_API int nb_insert_and_extract_central_slices_3d(
     const nb_transform* output_inv_scaling, const nb_transform* output_fwd_rotation,
     const nb_options* options, void* stream);
 
+/* No counterpart in the reference. Same arguments, checks and results as
+ * nb_rasterize_central_slices_3d, but the call allocates no device memory: for callers that cannot let
+ * a library allocate at call time (a fixed up-front memory budget, an allocator owned by someone else,
+ * a steady state that must not enter the driver's allocator). With output weights, the (value, weight)
+ * accumulator lives in a 64 MiB array this library reserves on every GPU that loads it, until exit, so
+ * the rfft grid D*H*(W/2+1) may hold at most 4,194,304 voxels for complex values (8,388,608 for real
+ * ones); larger volumes return NB_ERROR_INVALID. The first call on a device looks the array up (make
+ * it before any stream capture). All calls share the array and each clears the part it uses first:
+ * calls that overlap on the GPU race, so order them. */
+NB_API int nb_rasterize_central_slices_3d_static_scratch(
+    int32_t remap,
+    const nb_array* slice, const nb_array* slice_weight, const int64_t slice_shape[4],
+    const nb_array* volume, const nb_array* volume_weight, const int64_t volume_shape[4],
+    const nb_transform* inv_scaling, const nb_transform* fwd_rotation,
+    const nb_options* options, void* stream);
+
 /* Description of the last error on the calling thread ("" if none). */
 NB_API const char* nb_last_error(void);
 

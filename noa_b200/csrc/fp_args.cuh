@@ -4,6 +4,7 @@
 #pragma once
 
 #include "fp_common.cuh"
+#include "noa_b200/fourier_project.h"
 
 namespace nb {
 
@@ -42,6 +43,18 @@ cudaError_t launch_extract(const ProjArgs& a, cudaStream_t stream);
 cudaError_t launch_rasterize(const ProjArgs& a, cudaStream_t stream);
 cudaError_t launch_insert(const ProjArgs& a, cudaStream_t stream);
 cudaError_t launch_insert_extract(const ProjArgs& a, cudaStream_t stream);
+
+// Argument checks and per-call constants of nb_rasterize_central_slices_3d (capi.cu); fills `a` and
+// returns NB_OK, or an NB_ERROR_* code with the thread's last-error message set.
+int prepare_rasterize(int32_t remap,
+                      const nb_array* slice, const nb_array* slice_weight, const int64_t slice_shape[4],
+                      const nb_array* volume, const nb_array* volume_weight, const int64_t volume_shape[4],
+                      const nb_transform* inv_scaling, const nb_transform* fwd_rotation,
+                      const nb_options* options, ProjArgs& a);
+// NB_OK (clearing the thread's last error) or NB_ERROR_CUDA with the launch error's description.
+int finish_launch(cudaError_t err);
+// Sets the thread's last error and returns `code`.
+int report_error(int code, const char* message);
 
 // Number of SMs of the current device (cached per device).
 int sm_count();

@@ -70,11 +70,14 @@ def lib() -> C.CDLL:
         arr, xf, opt = P(NbArray), P(NbTransform), P(NbOptions)
         shape = P(C.c_int64)
         h.nb_rasterize_central_slices_3d.argtypes = [C.c_int32, arr, arr, shape, arr, arr, shape, xf, xf, opt, C.c_void_p]
+        h.nb_rasterize_central_slices_3d_static_scratch.argtypes = [C.c_int32, arr, arr, shape, arr, arr, shape, xf, xf,
+                                                                   opt, C.c_void_p]
         h.nb_insert_central_slices_3d.argtypes = [C.c_int32, arr, arr, shape, arr, arr, shape, xf, xf, opt, C.c_void_p]
         h.nb_extract_central_slices_3d.argtypes = [C.c_int32, arr, arr, shape, arr, arr, shape, xf, xf, opt, C.c_void_p]
         h.nb_insert_and_extract_central_slices_3d.argtypes = [C.c_int32, arr, arr, shape, arr, arr, shape,
                                                                xf, xf, xf, xf, opt, C.c_void_p]
-        for f in ("nb_rasterize_central_slices_3d", "nb_insert_central_slices_3d",
+        for f in ("nb_rasterize_central_slices_3d", "nb_rasterize_central_slices_3d_static_scratch",
+                  "nb_insert_central_slices_3d",
                   "nb_extract_central_slices_3d", "nb_insert_and_extract_central_slices_3d"):
             getattr(h, f).restype = C.c_int
         h.nb_last_error.restype = C.c_char_p
@@ -239,6 +242,24 @@ def rasterize_central_slices_3d(remap: str, slice, slice_weight, slice_shape, vo
     keep = []
     o = _options(fftfreq_cutoff=fftfreq_cutoff, target_shape=target_shape, ews_radius=ews_radius)
     _check(lib().nb_rasterize_central_slices_3d(
+        REMAPS[remap], _ref(as_nb_array(slice, keep)), _ref(as_nb_array(slice_weight, keep)), _shape(slice_shape),
+        _ref(as_nb_array(volume, keep)), _ref(as_nb_array(volume_weight, keep)), _shape(volume_shape),
+        _ref(as_nb_transform(inv_scaling, False, keep)), _ref(as_nb_transform(fwd_rotation, True, keep)),
+        C.byref(o), _stream_ptr(stream)))
+
+
+def rasterize_central_slices_3d_static_scratch(remap: str, slice, slice_weight, slice_shape, volume, volume_weight,
+                                               volume_shape, inv_scaling, fwd_rotation, *, fftfreq_cutoff=0.5,
+                                               target_shape=None, ews_radius=(0.0, 0.0), stream=None) -> None:
+    """rasterize_central_slices_3d without any device allocation (no counterpart in the reference).
+
+    For callers that cannot let the library allocate device memory at call time. The accumulator is a
+    64 MiB array reserved per GPU when the library loads: with weights, volumes up to 4,194,304 rfft
+    voxels (complex) are accepted, larger ones raise. Calls share that array, so calls that overlap on
+    the GPU must be ordered; the first call on a device should come before any stream capture."""
+    keep = []
+    o = _options(fftfreq_cutoff=fftfreq_cutoff, target_shape=target_shape, ews_radius=ews_radius)
+    _check(lib().nb_rasterize_central_slices_3d_static_scratch(
         REMAPS[remap], _ref(as_nb_array(slice, keep)), _ref(as_nb_array(slice_weight, keep)), _shape(slice_shape),
         _ref(as_nb_array(volume, keep)), _ref(as_nb_array(volume_weight, keep)), _shape(volume_shape),
         _ref(as_nb_transform(inv_scaling, False, keep)), _ref(as_nb_transform(fwd_rotation, True, keep)),
