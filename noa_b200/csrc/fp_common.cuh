@@ -547,6 +547,32 @@ __device__ __forceinline__ float2 dst_load(const DstView& d, int64_t i0, int64_t
         return make_float2(static_cast<const float*>(d.data)[off], 0.f);
 }
 
+// Streaming (evict-first) variants, for data touched once per launch (output slices, input slices),
+// so that it does not push the reused working set (volume, accumulator) out of L2.
+template<bool CPLX>
+__device__ __forceinline__ void dst_store_stream(const DstView& d, int64_t i0, int64_t i1, int64_t i2, float2 v) {
+    const int64_t off = i0 * d.s0 + i1 * d.s1 + i2 * d.s2;
+    if constexpr (CPLX)
+        __stcs(static_cast<float2*>(d.data) + off, v);
+    else
+        __stcs(static_cast<float*>(d.data) + off, v.x);
+}
+
+__device__ __forceinline__ void store_real_stream(const DstView& d, int64_t i0, int64_t i1, int64_t i2, float v) {
+    __stcs(static_cast<float*>(d.data) + (i0 * d.s0 + i1 * d.s1 + i2 * d.s2), v);
+}
+
+template<bool CPLX>
+__device__ __forceinline__ float2 src_read_stream(const SrcView& s, int64_t i0, int64_t i1, int64_t i2) {
+    if (s.is_value)
+        return s.value;
+    const int64_t off = i0 * s.s0 + i1 * s.s1 + i2 * s.s2;
+    if constexpr (CPLX)
+        return __ldcs(static_cast<const float2*>(s.data) + off);
+    else
+        return make_float2(__ldcs(static_cast<const float*>(s.data) + off), 0.f);
+}
+
 __device__ __forceinline__ void store_real(const DstView& d, int64_t i0, int64_t i1, int64_t i2, float v) {
     static_cast<float*>(d.data)[i0 * d.s0 + i1 * d.s1 + i2 * d.s2] = v;
 }

@@ -126,9 +126,9 @@ extract_pairs_kernel(const __grid_constant__ ProjArgs a, const float4* __restric
             const int y = y0 + r * TY;
             if (y >= a.slice_h)
                 continue;
-            dst_store<OUT_C>(a.out, b, y, u, value[r]);
+            dst_store_stream<OUT_C>(a.out, b, y, u, value[r]);
             if (has_out_w)
-                store_real(a.out_w, b, y, u, inside[r] ? 1.f : 0.f);
+                store_real_stream(a.out_w, b, y, u, inside[r] ? 1.f : 0.f);
         }
     }
 }
@@ -215,9 +215,9 @@ extract_kernel(const __grid_constant__ ProjArgs a, int ntx) {
                 }
             }
         }
-        dst_store<OUT_C>(a.out, b, y, u, value);
+        dst_store_stream<OUT_C>(a.out, b, y, u, value);
         if (has_out_w)
-            store_real(a.out_w, b, y, u, weight);
+            store_real_stream(a.out_w, b, y, u, weight);
     }
 }
 

@@ -70,7 +70,7 @@ rasterize_kernel(const __grid_constant__ ProjArgs a, int ntx, void* scratch) {
         }
         const float q0 = mul(fz, a.target0), q1 = mul(fy, a.target1), q2 = mul(fx, a.target2);
 
-        float2 value = src_read<IN_C>(a.in, b, y, u);
+        float2 value = src_read_stream<IN_C>(a.in, b, y, u);
         if constexpr (IN_C && OUT_C)
             value = cmul(value, conjugate); // noa multiplies by -1 here, it does not conjugate
         else

@@ -9,9 +9,9 @@
 // driver's allocator in its steady state. This entry point serves them.
 //
 // Limits and rules:
-//   * The accumulator is a file-scope __device__ array of NB_STATIC_SCRATCH_BYTES (64 MiB), held on
+//   * The accumulator is a file-scope __device__ array of STATIC_SCRATCH_BYTES (64 MiB), held on
 //     every GPU that loads this library until the process exits. With output weights, volumes up to
-//     NB_STATIC_SCRATCH_BYTES / 16 voxels (complex values) or / 8 voxels (real values) of the rfft grid
+//     STATIC_SCRATCH_BYTES / 16 voxels (complex values) or / 8 voxels (real values) of the rfft grid
 //     (D * H * (W/2+1)) are accepted; larger volumes are rejected with NB_ERROR_INVALID. Without output
 //     weights the reductions go straight into the caller's grid and no scratch is used at all.
 //   * The first call on a device looks up the array's device address (cudaGetSymbolAddress, with that
