@@ -1,0 +1,65 @@
+/* noa_b200 — batched extraction: many extract_central_slices_3d calls in one persistent launch.
+ *
+ * No single function of the reference corresponds to this: it executes a list of
+ * extract_central_slices_3d calls (noa/xform/FourierProject.hpp:1869-1914) — different volumes, box
+ * sizes and slice counts — as ONE persistent kernel fed by a device work queue, captured once into a
+ * CUDA graph and replayed. Every request is validated like nb_extract_central_slices_3d and produces
+ * bit-identical results. All requests of a batch share `remap` and `options`; their value types
+ * (c32->c32, c32->f32 or f32->f32) must agree; each volume must span fewer than 2^31 elements.
+ */
+#ifndef NOA_B200_BATCH_H
+#define NOA_B200_BATCH_H
+
+#include "noa_b200/fourier_project.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* One extraction: the arguments of nb_extract_central_slices_3d. The structs are read during
+ * nb_extract_batch_create; the device buffers they point to must stay valid while the batch is used. */
+typedef struct {
+    const nb_array* volume;
+    const nb_array* volume_weight;     /* nullable */
+    int64_t volume_shape[4];
+    const nb_array* slice;
+    const nb_array* slice_weight;      /* nullable */
+    int64_t slice_shape[4];
+    const nb_transform* inv_scaling;   /* nullable */
+    const nb_transform* fwd_rotation;
+} nb_extract_request;
+
+typedef struct nb_extract_batch_t* nb_extract_batch;
+
+/* Launch configuration of a batch (tile of pixels per work item, CTAs per SM, grid). */
+typedef struct {
+    int64_t n_requests;
+    int64_t n_items;       /* (slice, tile) work items */
+    int32_t tile_h, tile_w;
+    int32_t blocks_per_sm;
+    int32_t grid;
+    double tuned_ms;       /* time of the chosen configuration while autotuning, or -1 */
+    int32_t from_cache;    /* 1 if the configuration came from the autotune cache */
+} nb_batch_info;
+
+enum { NB_BATCH_AUTOTUNE = 1 };
+
+/* Validates the requests, uploads their descriptors, chooses the launch configuration (with
+ * NB_BATCH_AUTOTUNE: by timing the candidates on this batch, once per workload key, cached in memory and
+ * in the text file $NB_AUTOTUNE_CACHE or $HOME/.cache/noa_b200/autotune.txt; autotuning runs the batch,
+ * so it writes the outputs) and captures the launch into a CUDA graph. Synchronizes `stream`. */
+NB_API int nb_extract_batch_create(int32_t remap, const nb_extract_request* requests, int64_t n_requests,
+                                   const nb_options* options, int32_t flags, void* stream,
+                                   nb_extract_batch* batch);
+
+/* Replays the batch on `stream` (asynchronous). Calls on one batch must not overlap on the GPU. */
+NB_API int nb_extract_batch_run(nb_extract_batch batch, void* stream);
+
+NB_API int nb_extract_batch_info(nb_extract_batch batch, nb_batch_info* info);
+
+NB_API int nb_extract_batch_destroy(nb_extract_batch batch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,117 @@
+"""Batched extraction (Python side of include/noa_b200/batch.h).
+
+``ExtractBatch`` takes a list of extract_central_slices_3d calls — any mix of volumes, box sizes and
+slice counts — and runs them as one persistent kernel captured in a CUDA graph. Build it once, then
+``run()`` it as often as needed; the tensors it was given must stay alive and unchanged in shape.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+from . import fourier_project as fp
+
+
+class NbExtractRequest(C.Structure):
+    _fields_ = [("volume", C.POINTER(fp.NbArray)), ("volume_weight", C.POINTER(fp.NbArray)),
+                ("volume_shape", C.c_int64 * 4), ("slice", C.POINTER(fp.NbArray)),
+                ("slice_weight", C.POINTER(fp.NbArray)), ("slice_shape", C.c_int64 * 4),
+                ("inv_scaling", C.POINTER(fp.NbTransform)), ("fwd_rotation", C.POINTER(fp.NbTransform))]
+
+
+class NbBatchInfo(C.Structure):
+    _fields_ = [("n_requests", C.c_int64), ("n_items", C.c_int64), ("tile_h", C.c_int32), ("tile_w", C.c_int32),
+                ("blocks_per_sm", C.c_int32), ("grid", C.c_int32), ("tuned_ms", C.c_double),
+                ("from_cache", C.c_int32)]
+
+
+NB_BATCH_AUTOTUNE = 1
+
+
+@dataclass
+class ExtractRequest:
+    """The arguments of one extract_central_slices_3d call."""
+    volume: object
+    volume_shape: tuple
+    slice: object
+    slice_shape: tuple
+    fwd_rotation: object
+    inv_scaling: object = None
+    volume_weight: object = None
+    slice_weight: object = None
+
+
+def _setup(lib):
+    if getattr(lib, "_nb_batch_ready", False):
+        return
+    lib.nb_extract_batch_create.argtypes = [C.c_int32, C.POINTER(NbExtractRequest), C.c_int64,
+                                            C.POINTER(fp.NbOptions), C.c_int32, C.c_void_p,
+                                            C.POINTER(C.c_void_p)]
+    lib.nb_extract_batch_create.restype = C.c_int
+    lib.nb_extract_batch_run.argtypes = [C.c_void_p, C.c_void_p]
+    lib.nb_extract_batch_run.restype = C.c_int
+    lib.nb_extract_batch_info.argtypes = [C.c_void_p, C.POINTER(NbBatchInfo)]
+    lib.nb_extract_batch_info.restype = C.c_int
+    lib.nb_extract_batch_destroy.argtypes = [C.c_void_p]
+    lib.nb_extract_batch_destroy.restype = C.c_int
+    lib._nb_batch_ready = True
+
+
+class ExtractBatch:
+    """A captured batch of extractions. ``autotune=True`` times tile shapes and CTAs per SM on this
+    batch (once per workload key; the choice is cached) before capturing the launch."""
+
+    def __init__(self, remap: str, requests: list[ExtractRequest], *, interp="linear", fftfreq_cutoff=0.5,
+                 w_windowed_sinc=None, ews_radius=(0.0, 0.0), autotune=True, stream=None):
+        lib = fp.lib()
+        _setup(lib)
+        self._lib = lib
+        self._handle = None
+        self._keep = []
+        reqs = (NbExtractRequest * len(requests))()
+        for i, r in enumerate(requests):
+            q = reqs[i]
+            arrays = [fp.as_nb_array(t, self._keep) for t in (r.volume, r.volume_weight, r.slice, r.slice_weight)]
+            self._keep.extend(a for a in arrays if a is not None)
+            q.volume = C.pointer(arrays[0])
+            q.volume_weight = C.pointer(arrays[1]) if arrays[1] is not None else None
+            q.slice = C.pointer(arrays[2])
+            q.slice_weight = C.pointer(arrays[3]) if arrays[3] is not None else None
+            for k in range(4):
+                q.volume_shape[k] = int(r.volume_shape[k])
+                q.slice_shape[k] = int(r.slice_shape[k])
+            sc = fp.as_nb_transform(r.inv_scaling, False, self._keep)
+            rot = fp.as_nb_transform(r.fwd_rotation, True, self._keep)
+            self._keep.extend([sc, rot])
+            q.inv_scaling = C.pointer(sc)
+            q.fwd_rotation = C.pointer(rot)
+        self._keep.append(reqs)
+        opts = fp._options(interp=interp, fftfreq_cutoff=fftfreq_cutoff, ews_radius=ews_radius,
+                           w_windowed_sinc=w_windowed_sinc)
+        handle = C.c_void_p()
+        code = lib.nb_extract_batch_create(fp.REMAPS[remap], reqs, len(requests), C.byref(opts),
+                                           NB_BATCH_AUTOTUNE if autotune else 0, fp._stream_ptr(stream),
+                                           C.byref(handle))
+        fp._check(code)
+        self._handle = handle
+
+    def run(self, stream=None) -> None:
+        fp._check(self._lib.nb_extract_batch_run(self._handle, fp._stream_ptr(stream)))
+
+    def info(self) -> dict:
+        i = NbBatchInfo()
+        fp._check(self._lib.nb_extract_batch_info(self._handle, C.byref(i)))
+        return {"n_requests": i.n_requests, "n_items": i.n_items, "tile": (i.tile_h, i.tile_w),
+                "blocks_per_sm": i.blocks_per_sm, "grid": i.grid, "tuned_ms": i.tuned_ms,
+                "from_cache": bool(i.from_cache)}
+
+    def close(self) -> None:
+        if getattr(self, "_handle", None):
+            self._lib.nb_extract_batch_destroy(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -51,6 +51,12 @@ int prepare_rasterize(int32_t remap,
                       const nb_array* volume, const nb_array* volume_weight, const int64_t volume_shape[4],
                       const nb_transform* inv_scaling, const nb_transform* fwd_rotation,
                       const nb_options* options, ProjArgs& a);
+// Same for nb_extract_central_slices_3d.
+int prepare_extract(int32_t remap,
+                    const nb_array* volume, const nb_array* volume_weight, const int64_t volume_shape[4],
+                    const nb_array* slice, const nb_array* slice_weight, const int64_t slice_shape[4],
+                    const nb_transform* inv_scaling, const nb_transform* fwd_rotation,
+                    const nb_options* options, ProjArgs& a);
 // NB_OK (clearing the thread's last error) or NB_ERROR_CUDA with the launch error's description.
 int finish_launch(cudaError_t err);
 // Sets the thread's last error and returns `code`.

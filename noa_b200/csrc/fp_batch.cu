@@ -1,0 +1,482 @@
+// Batched extraction: many extract_central_slices_3d calls — different volumes, box sizes and slice
+// counts — executed by ONE persistent kernel, replayed as a CUDA graph.
+//
+// Work decomposition: every request is cut into (slice, tile) items, a tile being TY x TX pixels of
+// one output slice. Items are numbered request after request; a device counter hands them out, one
+// per CTA at a time (atomicAdd), so uneven requests balance themselves across the SMs without a
+// per-request launch. Each item runs the same per-pixel code as nb_extract_central_slices_3d's
+// generic path (extract_one below restates that kernel body for a single pixel), so results are
+// bit-identical to the per-call entry point.
+//
+// nb_extract_batch_create validates every request like the per-call entry point, uploads the request
+// descriptors once, optionally autotunes (tile shape x CTAs per SM, timed on the batch itself and
+// cached per workload key in memory and in a small text file), and captures the launch — counter
+// reset + persistent kernel — into a CUDA graph. nb_extract_batch_run replays that graph on a stream.
+#include "fp_args.cuh"
+#include "noa_b200/batch.h"
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
+#include <map>
+#include <mutex>
+#include <set>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include <sys/stat.h>
+
+namespace nb {
+namespace {
+
+struct BatchReq {
+    ProjArgs a;
+    int ntx;                  // tiles along u
+    int tiles_per_slice;
+    int64_t first_item;       // index of this request's first item
+};
+
+// One output pixel (b, y, u) of request `a`: the body of extract_kernel (fp_extract.cu), with 32-bit
+// volume offsets (batches require volumes addressable in 31 bits).
+template<int I, bool IN_C, bool OUT_C>
+__device__ __forceinline__ void extract_one(const ProjArgs& a, int64_t b, int y, int u) {
+    const Spectrum3 sp{a.vol_d, a.vol_h, a.vol_w, a.in_centered};
+    const View3<int> vol{a.in.data, static_cast<int>(a.in.s0), static_cast<int>(a.in.s1), static_cast<int>(a.in.s2)};
+    const View3<int> volw{a.in_w.data, static_cast<int>(a.in_w.s0), static_cast<int>(a.in_w.s1),
+                          static_cast<int>(a.in_w.s2)};
+    const bool has_out_w = a.out_w.present;
+    const bool has_in_w = a.in_w.present;
+    const int v = index2frequency(a.out_centered, y, a.slice_h);
+    const float f0 = div(static_cast<float>(v), a.f_slice0);
+    const float f1 = div(static_cast<float>(u), a.f_slice1);
+    float fz, fy, fx;
+    slice2grid(f0, f1, a.scale, a.rot, b, a.ews, fz, fy, fx);
+    float2 value = make_float2(0.f, 0.f);
+    float weight = 0.f;
+    if (a.wsize <= 1) {
+        if (dot3(fz, fy, fx, fz, fy, fx) <= a.cutoff_sqd) {
+            const float q0 = mul(fz, a.target0), q1 = mul(fy, a.target1), q2 = mul(fx, a.target2);
+            value = to_output<IN_C, OUT_C>(interp_3d<I, IN_C>(vol, sp, q0, q1, q2));
+            if (has_out_w)
+                weight = has_in_w ? interp_3d<I, false>(volw, sp, q0, q1, q2).x : 1.f;
+        }
+    } else {
+        for (int w = 0; w < a.wsize; ++w) {
+            const float off = div(static_cast<float>(w - a.wsize / 2), a.target0);
+            const float gz = add(fz, off);
+            if (dot3(gz, fy, fx, gz, fy, fx) > a.cutoff_sqd)
+                continue;
+            const float q0 = mul(gz, a.target0), q1 = mul(fy, a.target1), q2 = mul(fx, a.target2);
+            const float cw = windowed_sinc(off, a.efs, a.efb);
+            const float2 iv = to_output<IN_C, OUT_C>(interp_3d<I, IN_C>(vol, sp, q0, q1, q2));
+            value = cadd(value, cmul(iv, cw));
+            if (has_out_w) {
+                const float iw = has_in_w ? interp_3d<I, false>(volw, sp, q0, q1, q2).x : 1.f;
+                weight = add(weight, mul(iw, cw));
+            }
+        }
+    }
+    dst_store_stream<OUT_C>(a.out, b, y, u, value);
+    if (has_out_w)
+        store_real_stream(a.out_w, b, y, u, weight);
+}
+
+// Tile shapes of the autotuner. 256 threads; a warp covers WY x WX pixels.
+constexpr int N_VARIANTS = 2;
+struct Variant { int ty, tx, wy, wx; };
+constexpr Variant VARIANTS[N_VARIANTS] = {{16, 16, 4, 8}, {8, 32, 2, 16}};
+
+template<int I, bool IN_C, bool OUT_C, int V>
+__global__ void __launch_bounds__(256)
+batch_extract_kernel(const BatchReq* __restrict__ reqs, int n_req, int64_t n_items,
+                     unsigned long long* __restrict__ counter) {
+    constexpr Variant VT = VARIANTS[V];
+    __shared__ long long s_item;
+    __shared__ int s_req;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    constexpr int WARPS_X = VT.tx / VT.wx;
+    const int ly = (warp / WARPS_X) * VT.wy + lane / VT.wx;
+    const int lx = (warp % WARPS_X) * VT.wx + lane % VT.wx;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const long long item = static_cast<long long>(atomicAdd(counter, 1ull));
+            int lo = 0, hi = n_req - 1;
+            if (item < n_items) {
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) / 2;
+                    if (reqs[mid].first_item <= item)
+                        lo = mid;
+                    else
+                        hi = mid - 1;
+                }
+            }
+            s_item = item;
+            s_req = lo;
+        }
+        __syncthreads();
+        const long long item = s_item;
+        const int r = s_req;
+        __syncthreads();
+        if (item >= n_items)
+            break;
+        const BatchReq& R = reqs[r];
+        const int64_t local = item - R.first_item;
+        const int64_t b = local / R.tiles_per_slice;
+        const int tile = static_cast<int>(local - b * R.tiles_per_slice);
+        const int y = (tile / R.ntx) * VT.ty + ly;
+        const int u = (tile % R.ntx) * VT.tx + lx;
+        if (y < R.a.slice_h && u < R.a.slice_w / 2 + 1)
+            extract_one<I, IN_C, OUT_C>(R.a, b, y, u);
+    }
+}
+
+using KernelFn = void (*)(const BatchReq*, int, int64_t, unsigned long long*);
+
+template<int I, bool IN_C, bool OUT_C>
+KernelFn pick_v(int v) {
+    return v == 0 ? batch_extract_kernel<I, IN_C, OUT_C, 0> : batch_extract_kernel<I, IN_C, OUT_C, 1>;
+}
+
+template<int I>
+KernelFn pick_t(bool in_c, bool out_c, int v) {
+    if (in_c && out_c) return pick_v<I, true, true>(v);
+    if (in_c) return pick_v<I, true, false>(v);
+    return pick_v<I, false, false>(v);
+}
+
+KernelFn pick_kernel(int interp, bool in_c, bool out_c, int v) {
+    switch (interp) {
+        case I_NEAREST: return pick_t<I_NEAREST>(in_c, out_c, v);
+        case I_LINEAR: return pick_t<I_LINEAR>(in_c, out_c, v);
+        case I_CUBIC: return pick_t<I_CUBIC>(in_c, out_c, v);
+        case I_BSPLINE: return pick_t<I_BSPLINE>(in_c, out_c, v);
+        case I_LANCZOS4: return pick_t<I_LANCZOS4>(in_c, out_c, v);
+        case I_LANCZOS6: return pick_t<I_LANCZOS6>(in_c, out_c, v);
+        default: return pick_t<I_LANCZOS8>(in_c, out_c, v);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------
+// Autotune cache: "key variant blocks_per_sm ms" lines, in memory and in a text file
+// ($NB_AUTOTUNE_CACHE, else $HOME/.cache/noa_b200/autotune.txt).
+// ---------------------------------------------------------------------------------------------------
+std::mutex g_tune_mutex;
+std::map<std::string, std::pair<int, int>> g_tuned;
+std::string g_loaded_path;
+bool g_tune_loaded = false;
+
+std::string cache_path() {
+    if (const char* p = std::getenv("NB_AUTOTUNE_CACHE"))
+        return p;
+    if (const char* h = std::getenv("HOME"))
+        return std::string(h) + "/.cache/noa_b200/autotune.txt";
+    return "";
+}
+
+void load_cache_locked() {
+    const std::string path = cache_path();
+    if (g_tune_loaded && path == g_loaded_path)
+        return;
+    g_tune_loaded = true;
+    g_loaded_path = path;
+    g_tuned.clear();
+    if (path.empty())
+        return;
+    std::ifstream f(path);
+    std::string line;
+    while (std::getline(f, line)) {
+        std::istringstream is(line);
+        std::string key;
+        int v = 0, bps = 0;
+        double ms = 0;
+        if (is >> key >> v >> bps >> ms && v >= 0 && v < N_VARIANTS && bps > 0)
+            g_tuned[key] = {v, bps};
+    }
+}
+
+void store_cache_locked(const std::string& key, int v, int bps, double ms) {
+    g_tuned[key] = {v, bps};
+    const std::string path = cache_path();
+    if (path.empty())
+        return;
+    const size_t slash = path.rfind('/');
+    if (slash != std::string::npos && slash > 0) {
+        const std::string dir = path.substr(0, slash);
+        for (size_t i = 1; i <= dir.size(); ++i) {
+            if (i == dir.size() || dir[i] == '/')
+                mkdir(dir.substr(0, i).c_str(), 0755);  // existing levels fail harmlessly
+        }
+    }
+    std::ofstream f(path, std::ios::app);
+    if (f)
+        f << key << ' ' << v << ' ' << bps << ' ' << ms << '\n';
+}
+
+struct Config {
+    int variant;
+    int blocks_per_sm;
+};
+
+} // namespace
+} // namespace nb
+
+using namespace nb;
+
+struct nb_extract_batch_t {
+    int device = 0;
+    int interp = 1;
+    bool in_cplx = true, out_cplx = true;
+    std::vector<BatchReq> host_reqs;     // ProjArgs of every request; tile fields per variant
+    BatchReq* d_reqs = nullptr;
+    unsigned long long* d_counter = nullptr;
+    int64_t n_items = 0;
+    Config cfg{0, 1};
+    int grid = 0;
+    double tuned_ms = -1;
+    bool from_cache = false;
+    std::string key;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+namespace nb {
+namespace {
+
+int max_blocks_per_sm(KernelFn fn) {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, 256, 0) != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    return n > 0 ? n : 1;
+}
+
+// Fills the per-variant tile fields and uploads the descriptors.
+cudaError_t upload(nb_extract_batch_t* h, int variant, cudaStream_t stream) {
+    const Variant vt = VARIANTS[variant];
+    int64_t first = 0;
+    for (BatchReq& r : h->host_reqs) {
+        const int wp = r.a.slice_w / 2 + 1;
+        r.ntx = (wp + vt.tx - 1) / vt.tx;
+        r.tiles_per_slice = r.ntx * ((r.a.slice_h + vt.ty - 1) / vt.ty);
+        r.first_item = first;
+        first += static_cast<int64_t>(r.tiles_per_slice) * r.a.n_slices;
+    }
+    h->n_items = first;
+    cudaError_t err = cudaMemcpyAsync(h->d_reqs, h->host_reqs.data(), h->host_reqs.size() * sizeof(BatchReq),
+                                      cudaMemcpyHostToDevice, stream);
+    if (err != cudaSuccess)
+        return err;
+    return cudaStreamSynchronize(stream);
+}
+
+cudaError_t launch(nb_extract_batch_t* h, const Config& c, cudaStream_t stream) {
+    const KernelFn fn = pick_kernel(h->interp, h->in_cplx, h->out_cplx, c.variant);
+    const int grid = sm_count() * c.blocks_per_sm;
+    cudaError_t err = cudaMemsetAsync(h->d_counter, 0, sizeof(unsigned long long), stream);
+    if (err != cudaSuccess)
+        return err;
+    fn<<<grid, 256, 0, stream>>>(h->d_reqs, static_cast<int>(h->host_reqs.size()), h->n_items, h->d_counter);
+    return cudaGetLastError();
+}
+
+// Median of `reps` timed launches (after one warm-up), in milliseconds.
+double time_config(nb_extract_batch_t* h, const Config& c, cudaStream_t stream, int reps) {
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    std::vector<float> t;
+    double result = 1e30;
+    if (launch(h, c, stream) == cudaSuccess && cudaStreamSynchronize(stream) == cudaSuccess) {
+        for (int i = 0; i < reps; ++i) {
+            cudaEventRecord(e0, stream);
+            if (launch(h, c, stream) != cudaSuccess)
+                break;
+            cudaEventRecord(e1, stream);
+            if (cudaEventSynchronize(e1) != cudaSuccess)
+                break;
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            t.push_back(ms);
+        }
+        if (!t.empty()) {
+            std::sort(t.begin(), t.end());
+            result = t[t.size() / 2];
+        }
+    }
+    cudaGetLastError();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return result;
+}
+
+std::string workload_key(const nb_extract_batch_t* h) {
+    std::set<std::string> boxes;
+    int64_t slices = 0;
+    for (const BatchReq& r : h->host_reqs) {
+        boxes.insert(std::to_string(r.a.vol_d) + "x" + std::to_string(r.a.vol_h) + "x" + std::to_string(r.a.vol_w));
+        slices += r.a.n_slices;
+    }
+    std::ostringstream k;
+    k << "extract/i" << h->interp << "/t" << h->in_cplx << h->out_cplx << "/sm" << sm_count() << "/b";
+    for (const std::string& b : boxes)
+        k << b << ',';
+    int64_t bucket = 1;
+    while (bucket < slices)
+        bucket *= 2;
+    k << "/s" << bucket;
+    return k.str();
+}
+
+void release(nb_extract_batch_t* h) {
+    if (!h)
+        return;
+    if (h->exec) cudaGraphExecDestroy(h->exec);
+    if (h->graph) cudaGraphDestroy(h->graph);
+    if (h->d_reqs) cudaFree(h->d_reqs);
+    if (h->d_counter) cudaFree(h->d_counter);
+    delete h;
+}
+
+} // namespace
+} // namespace nb
+
+extern "C" {
+
+int nb_extract_batch_create(int32_t remap, const nb_extract_request* requests, int64_t n_requests,
+                            const nb_options* options, int32_t flags, void* stream, nb_extract_batch* out) {
+    if (!out)
+        return report_error(NB_ERROR_INVALID, "out should not be NULL");
+    *out = nullptr;
+    if (!requests || n_requests <= 0)
+        return report_error(NB_ERROR_INVALID, "a batch needs at least one request");
+    if (n_requests > (int64_t(1) << 30))
+        return report_error(NB_ERROR_INVALID, "too many requests");
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    auto* h = new nb_extract_batch_t();
+    cudaGetDevice(&h->device);
+    h->host_reqs.resize(static_cast<size_t>(n_requests));
+    for (int64_t i = 0; i < n_requests; ++i) {
+        const nb_extract_request& q = requests[i];
+        ProjArgs a{};
+        const int st = prepare_extract(remap, q.volume, q.volume_weight, q.volume_shape, q.slice, q.slice_weight,
+                                       q.slice_shape, q.inv_scaling, q.fwd_rotation, options, a);
+        if (st != NB_OK) {
+            release(h);
+            return st;
+        }
+        if (a.wide_in) {
+            release(h);
+            return report_error(NB_ERROR_INVALID, "batched volumes must span fewer than 2^31 elements");
+        }
+        if (i == 0) {
+            h->interp = a.interp;
+            h->in_cplx = a.in_cplx;
+            h->out_cplx = a.out_cplx;
+        } else if (a.in_cplx != h->in_cplx || a.out_cplx != h->out_cplx) {
+            release(h);
+            return report_error(NB_ERROR_INVALID, "all requests of a batch must have the same value types");
+        }
+        h->host_reqs[static_cast<size_t>(i)].a = a;
+    }
+    if (cudaMalloc(&h->d_reqs, h->host_reqs.size() * sizeof(BatchReq)) != cudaSuccess ||
+        cudaMalloc(&h->d_counter, sizeof(unsigned long long)) != cudaSuccess) {
+        cudaGetLastError();
+        release(h);
+        return report_error(NB_ERROR_OOM, "cannot allocate the batch descriptors");
+    }
+
+    // Configuration: autotuned (cached per workload key), or the default.
+    h->key = workload_key(h);
+    Config best{0, max_blocks_per_sm(pick_kernel(h->interp, h->in_cplx, h->out_cplx, 0))};
+    bool tuned = false;
+    if (flags & NB_BATCH_AUTOTUNE) {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        load_cache_locked();
+        auto it = g_tuned.find(h->key);
+        if (it != g_tuned.end()) {
+            best = {it->second.first, it->second.second};
+            h->from_cache = true;
+            tuned = true;
+        }
+    }
+    if ((flags & NB_BATCH_AUTOTUNE) && !tuned) {
+        double best_ms = 1e30;
+        for (int v = 0; v < N_VARIANTS; ++v) {
+            if (upload(h, v, s) != cudaSuccess)
+                continue;
+            const int max_b = max_blocks_per_sm(pick_kernel(h->interp, h->in_cplx, h->out_cplx, v));
+            const std::set<int> cands{1, 2, 4, max_b};
+            for (int bps : cands) {
+                if (bps > max_b)
+                    continue;
+                const double ms = time_config(h, Config{v, bps}, s, 3);
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best = {v, bps};
+                }
+            }
+        }
+        h->tuned_ms = best_ms;
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        store_cache_locked(h->key, best.variant, best.blocks_per_sm, best_ms);
+    }
+    h->cfg = best;
+    cudaError_t err = upload(h, best.variant, s);
+    if (err != cudaSuccess) {
+        release(h);
+        return finish_launch(err);
+    }
+    h->grid = sm_count() * best.blocks_per_sm;
+
+    // Capture counter reset + persistent kernel into a graph, on a private stream.
+    cudaStream_t cap;
+    if ((err = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking)) == cudaSuccess) {
+        err = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+        if (err == cudaSuccess) {
+            const cudaError_t lerr = launch(h, best, cap);
+            err = cudaStreamEndCapture(cap, &h->graph);
+            if (err == cudaSuccess && lerr != cudaSuccess)
+                err = lerr;
+        }
+        if (err == cudaSuccess)
+            err = cudaGraphInstantiate(&h->exec, h->graph, 0);
+        cudaStreamDestroy(cap);
+    }
+    if (err != cudaSuccess) {
+        release(h);
+        return finish_launch(err);
+    }
+    *out = h;
+    return finish_launch(cudaSuccess);
+}
+
+int nb_extract_batch_run(nb_extract_batch batch, void* stream) {
+    if (!batch || !batch->exec)
+        return report_error(NB_ERROR_INVALID, "invalid batch handle");
+    return finish_launch(cudaGraphLaunch(batch->exec, static_cast<cudaStream_t>(stream)));
+}
+
+int nb_extract_batch_info(nb_extract_batch batch, nb_batch_info* info) {
+    if (!batch || !info)
+        return report_error(NB_ERROR_INVALID, "invalid batch handle");
+    const Variant vt = VARIANTS[batch->cfg.variant];
+    info->n_requests = static_cast<int64_t>(batch->host_reqs.size());
+    info->n_items = batch->n_items;
+    info->tile_h = vt.ty;
+    info->tile_w = vt.tx;
+    info->blocks_per_sm = batch->cfg.blocks_per_sm;
+    info->grid = batch->grid;
+    info->tuned_ms = batch->tuned_ms;
+    info->from_cache = batch->from_cache;
+    return NB_OK;
+}
+
+int nb_extract_batch_destroy(nb_extract_batch batch) {
+    release(batch);
+    return NB_OK;
+}
+
+} // extern "C"
