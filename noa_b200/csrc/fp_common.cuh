@@ -355,6 +355,22 @@ __device__ __forceinline__ float2 interp_spectrum_2d(const SrcView& src, const S
         interp_weights<I>(sub(f0, fl0), w0);
         interp_weights<I>(sub(f1, fl1), w1);
         float2 value = make_float2(0.f, 0.f);
+        if constexpr (SIZE > 2) {
+            // Interior fast path (all taps in bounds, none flipped): same terms, same order.
+            constexpr int END = SIZE / 2;
+            if (b0 + START >= lo0 && b0 + END <= hi0 && b1 + START >= 0 && b1 + END <= hi1) {
+#pragma unroll
+                for (int y = 0; y < SIZE; ++y) {
+                    const int iy = frequency2index(sp.centered, b0 + START + y, sp.n0);
+                    float2 vy = make_float2(0.f, 0.f);
+#pragma unroll
+                    for (int x = 0; x < SIZE; ++x)
+                        vy = cfma(src_read<CPLX>(src, batch, iy, b1 + START + x), w1[x], vy);
+                    value = cfma(vy, w0[y], value);
+                }
+                return value;
+            }
+        }
 #pragma unroll
         for (int y = 0; y < SIZE; ++y) {
             float2 vy = make_float2(0.f, 0.f);
@@ -485,10 +501,34 @@ __device__ __forceinline__ float2 interp_3d(const View3<Idx>& v, const Spectrum3
             interp_weights<I>(sub(f1, fl1), w1);
             interp_weights<I>(sub(f2, fl2), w2);
             float2 value = make_float2(0.f, 0.f);
+            constexpr int END = SIZE / 2;
+            // Interior fast path: every tap in bounds and on the stored half (no per-tap Friedel
+            // flip), so each (z, y) row of the window is SIZE consecutive x elements. Same terms in the
+            // same order as the general loop below, hence the same bits.
+            if (b0 + START >= lo0 && b0 + END <= hi0 && b1 + START >= lo1 && b1 + END <= hi1 &&
+                b2 + START >= 0 && b2 + END <= hi2) {
+                const Idx x0 = static_cast<Idx>(b2 + START) * v.s2;
 #pragma unroll (SIZE <= 4 ? SIZE : 1)
+                for (int z = 0; z < SIZE; ++z) {
+                    const Idx oz = static_cast<Idx>(frequency2index(sp.centered, b0 + START + z, sp.n0)) * v.s0 + x0;
+                    float2 vz = make_float2(0.f, 0.f);
+#pragma unroll
+                    for (int y = 0; y < SIZE; ++y) {
+                        const Idx row = oz + static_cast<Idx>(frequency2index(sp.centered, b1 + START + y, sp.n1)) * v.s1;
+                        float2 vy = make_float2(0.f, 0.f);
+#pragma unroll
+                        for (int x = 0; x < SIZE; ++x)
+                            vy = cfma(view_read<CPLX>(v, row + static_cast<Idx>(x) * v.s2), w2[x], vy);
+                        vz = cfma(vy, w1[y], vz);
+                    }
+                    value = cfma(vz, w0[z], value);
+                }
+                return value;
+            }
+#pragma unroll 1
             for (int z = 0; z < SIZE; ++z) {
                 float2 vz = make_float2(0.f, 0.f);
-#pragma unroll
+#pragma unroll (SIZE <= 4 ? SIZE : 1)
                 for (int y = 0; y < SIZE; ++y) {
                     float2 vy = make_float2(0.f, 0.f);
 #pragma unroll
