@@ -40,6 +40,7 @@ typedef struct {
     int32_t grid;
     double tuned_ms;       /* time of the chosen configuration while autotuning, or -1 */
     int32_t from_cache;    /* 1 if the configuration came from the autotune cache */
+    int32_t min_ctas;      /* CTAs per SM the kernel variant was compiled for (its register cap) */
 } nb_batch_info;
 
 enum { NB_BATCH_AUTOTUNE = 1 };

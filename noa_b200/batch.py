@@ -22,7 +22,7 @@ class NbExtractRequest(C.Structure):
 class NbBatchInfo(C.Structure):
     _fields_ = [("n_requests", C.c_int64), ("n_items", C.c_int64), ("tile_h", C.c_int32), ("tile_w", C.c_int32),
                 ("blocks_per_sm", C.c_int32), ("grid", C.c_int32), ("tuned_ms", C.c_double),
-                ("from_cache", C.c_int32)]
+                ("from_cache", C.c_int32), ("min_ctas", C.c_int32)]
 
 
 NB_BATCH_AUTOTUNE = 1
@@ -103,7 +103,7 @@ class ExtractBatch:
         fp._check(self._lib.nb_extract_batch_info(self._handle, C.byref(i)))
         return {"n_requests": i.n_requests, "n_items": i.n_items, "tile": (i.tile_h, i.tile_w),
                 "blocks_per_sm": i.blocks_per_sm, "grid": i.grid, "tuned_ms": i.tuned_ms,
-                "from_cache": bool(i.from_cache)}
+                "from_cache": bool(i.from_cache), "min_ctas": i.min_ctas}
 
     def close(self) -> None:
         if getattr(self, "_handle", None):

@@ -83,13 +83,15 @@ __device__ __forceinline__ void extract_one(const ProjArgs& a, int64_t b, int y,
         store_real_stream(a.out_w, b, y, u, weight);
 }
 
-// Tile shapes of the autotuner. 256 threads; a warp covers WY x WX pixels.
-constexpr int N_VARIANTS = 2;
-struct Variant { int ty, tx, wy, wx; };
-constexpr Variant VARIANTS[N_VARIANTS] = {{16, 16, 4, 8}, {8, 32, 2, 16}};
+// Kernel variants of the autotuner: tile shape (256 threads; a warp covers WY x WX pixels) and the
+// minimum resident CTAs per SM promised to the compiler (4 caps registers at 64 per thread, trading
+// spills of the wide stencils for twice the resident warps).
+constexpr int N_VARIANTS = 3;
+struct Variant { int ty, tx, wy, wx, min_ctas; };
+constexpr Variant VARIANTS[N_VARIANTS] = {{16, 16, 4, 8, 1}, {8, 32, 2, 16, 1}, {16, 16, 4, 8, 4}};
 
 template<int I, bool IN_C, bool OUT_C, int V>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, VARIANTS[V].min_ctas)
 batch_extract_kernel(const BatchReq* __restrict__ reqs, int n_req, int64_t n_items,
                      unsigned long long* __restrict__ counter) {
     constexpr Variant VT = VARIANTS[V];
@@ -136,7 +138,11 @@ using KernelFn = void (*)(const BatchReq*, int, int64_t, unsigned long long*);
 
 template<int I, bool IN_C, bool OUT_C>
 KernelFn pick_v(int v) {
-    return v == 0 ? batch_extract_kernel<I, IN_C, OUT_C, 0> : batch_extract_kernel<I, IN_C, OUT_C, 1>;
+    switch (v) {
+        case 0: return batch_extract_kernel<I, IN_C, OUT_C, 0>;
+        case 1: return batch_extract_kernel<I, IN_C, OUT_C, 1>;
+        default: return batch_extract_kernel<I, IN_C, OUT_C, 2>;
+    }
 }
 
 template<int I>
@@ -471,6 +477,7 @@ int nb_extract_batch_info(nb_extract_batch batch, nb_batch_info* info) {
     info->grid = batch->grid;
     info->tuned_ms = batch->tuned_ms;
     info->from_cache = batch->from_cache;
+    info->min_ctas = vt.min_ctas;
     return NB_OK;
 }
 
