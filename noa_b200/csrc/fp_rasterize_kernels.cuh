@@ -252,7 +252,7 @@ __device__ __forceinline__ unsigned slide_mask(unsigned m, bool up, bool dn) {
 }
 
 template<bool IN_C, bool OUT_C, bool W>
-__global__ void __launch_bounds__(RASTER_THREADS, 4)
+__global__ void __launch_bounds__(RASTER_THREADS, 3)
 rasterize_runs_kernel(const __grid_constant__ ProjArgs a, const AccGrid g, void* __restrict__ acc) {
     const int wp = a.slice_w / 2 + 1;
     const int t = blockIdx.x * RASTER_THREADS + threadIdx.x;
