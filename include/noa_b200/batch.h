@@ -58,6 +58,32 @@ NB_API int nb_extract_batch_run(nb_extract_batch batch, void* stream);
 
 NB_API int nb_extract_batch_info(nb_extract_batch batch, nb_batch_info* info);
 
+/* ---- Resident volumes and one-shot batched launches (used by serving loops) ----------------------- */
+
+/* Pair copy of a volume for LINEAR extraction: element (z, y, x) holds the x-neighbours v[z][y][x] and
+ * v[z][y][x+1] as 16 bytes, so a trilinear cell is four aligned loads. Results read through it are
+ * bit-identical to reading the volume. nb_volume_pairs_bytes gives its size (-1 for a bad shape);
+ * nb_volume_pairs writes it (`volume`: one c32 rfft volume, `volume_shape` {1, D, H, W}). */
+NB_API int64_t nb_volume_pairs_bytes(const int64_t volume_shape[4]);
+NB_API int nb_volume_pairs(const nb_array* volume, const int64_t volume_shape[4], void* pairs,
+                           int64_t pairs_bytes, void* stream);
+
+/* An extraction with, optionally, the pair copy of its volume. The copy is used where it applies
+ * (LINEAR, complex volume, no volume weights, no EWS, no scaling, no w-window) and ignored otherwise. */
+typedef struct {
+    nb_extract_request call;
+    const void* volume_pairs;          /* nullable */
+    int64_t volume_pairs_bytes;
+} nb_extract_request_ex;
+
+/* Validates the requests and enqueues them on `stream` as ONE persistent launch (no graph, no
+ * autotuning: the configuration cached for the workload key is used when there is one, else a default),
+ * staging the descriptors in stream-ordered device memory. The request structs may be freed on return;
+ * the device buffers must stay valid until the launch completes. Results are bit-identical to
+ * nb_extract_central_slices_3d on each request. */
+NB_API int nb_extract_batch_launch(int32_t remap, const nb_extract_request_ex* requests, int64_t n_requests,
+                                   const nb_options* options, void* stream);
+
 NB_API int nb_extract_batch_destroy(nb_extract_batch batch);
 
 #ifdef __cplusplus

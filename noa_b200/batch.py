@@ -19,6 +19,10 @@ class NbExtractRequest(C.Structure):
                 ("inv_scaling", C.POINTER(fp.NbTransform)), ("fwd_rotation", C.POINTER(fp.NbTransform))]
 
 
+class NbExtractRequestEx(C.Structure):
+    _fields_ = [("call", NbExtractRequest), ("volume_pairs", C.c_void_p), ("volume_pairs_bytes", C.c_int64)]
+
+
 class NbBatchInfo(C.Structure):
     _fields_ = [("n_requests", C.c_int64), ("n_items", C.c_int64), ("tile_h", C.c_int32), ("tile_w", C.c_int32),
                 ("blocks_per_sm", C.c_int32), ("grid", C.c_int32), ("tuned_ms", C.c_double),
@@ -54,7 +58,69 @@ def _setup(lib):
     lib.nb_extract_batch_info.restype = C.c_int
     lib.nb_extract_batch_destroy.argtypes = [C.c_void_p]
     lib.nb_extract_batch_destroy.restype = C.c_int
+    lib.nb_volume_pairs_bytes.argtypes = [C.POINTER(C.c_int64)]
+    lib.nb_volume_pairs_bytes.restype = C.c_int64
+    lib.nb_volume_pairs.argtypes = [C.POINTER(fp.NbArray), C.POINTER(C.c_int64), C.c_void_p, C.c_int64, C.c_void_p]
+    lib.nb_volume_pairs.restype = C.c_int
+    lib.nb_extract_batch_launch.argtypes = [C.c_int32, C.POINTER(NbExtractRequestEx), C.c_int64,
+                                            C.POINTER(fp.NbOptions), C.c_void_p]
+    lib.nb_extract_batch_launch.restype = C.c_int
     lib._nb_batch_ready = True
+
+
+def _fill_request(q: NbExtractRequest, r: ExtractRequest, keep: list) -> None:
+    arrays = [fp.as_nb_array(t, keep) for t in (r.volume, r.volume_weight, r.slice, r.slice_weight)]
+    keep.extend(a for a in arrays if a is not None)
+    q.volume = C.pointer(arrays[0])
+    q.volume_weight = C.pointer(arrays[1]) if arrays[1] is not None else None
+    q.slice = C.pointer(arrays[2])
+    q.slice_weight = C.pointer(arrays[3]) if arrays[3] is not None else None
+    for k in range(4):
+        q.volume_shape[k] = int(r.volume_shape[k])
+        q.slice_shape[k] = int(r.slice_shape[k])
+    sc = fp.as_nb_transform(r.inv_scaling, False, keep)
+    rot = fp.as_nb_transform(r.fwd_rotation, True, keep)
+    keep.extend([sc, rot])
+    q.inv_scaling = C.pointer(sc)
+    q.fwd_rotation = C.pointer(rot)
+
+
+def volume_pairs(volume, volume_shape, stream=None):
+    """The pair copy of one c32 rfft volume (1, D, H, W/2+1) for LINEAR extraction, as a uint8 device
+    tensor. Extractions given it (``extract_batch_launch``) read 4 aligned 16-byte pairs per pixel."""
+    torch = fp._torch()
+    lib = fp.lib()
+    _setup(lib)
+    shape = (C.c_int64 * 4)(*[int(x) for x in volume_shape])
+    nbytes = lib.nb_volume_pairs_bytes(shape)
+    if nbytes <= 0:
+        raise fp.NoaB200Error(fp.NB_ERROR_INVALID, f"bad volume shape {tuple(volume_shape)}")
+    pairs = torch.empty(int(nbytes), dtype=torch.uint8, device=volume.device)
+    keep = []
+    arr = fp.as_nb_array(volume, keep)
+    fp._check(lib.nb_volume_pairs(C.byref(arr), shape, pairs.data_ptr(), nbytes, fp._stream_ptr(stream)))
+    return pairs
+
+
+def extract_batch_launch(remap: str, requests: list[ExtractRequest], pairs: list | None = None, *,
+                         interp="linear", fftfreq_cutoff=0.5, w_windowed_sinc=None, ews_radius=(0.0, 0.0),
+                         stream=None) -> None:
+    """Enqueues many extract_central_slices_3d calls as ONE persistent launch on ``stream`` (no graph,
+    no autotuning). ``pairs[i]`` is an optional ``volume_pairs`` copy of request i's volume."""
+    lib = fp.lib()
+    _setup(lib)
+    keep = []
+    reqs = (NbExtractRequestEx * len(requests))()
+    for i, r in enumerate(requests):
+        _fill_request(reqs[i].call, r, keep)
+        p = pairs[i] if pairs is not None else None
+        if p is not None:
+            reqs[i].volume_pairs = p.data_ptr()
+            reqs[i].volume_pairs_bytes = p.numel() * p.element_size()
+    opts = fp._options(interp=interp, fftfreq_cutoff=fftfreq_cutoff, ews_radius=ews_radius,
+                       w_windowed_sinc=w_windowed_sinc)
+    fp._check(lib.nb_extract_batch_launch(fp.REMAPS[remap], reqs, len(requests), C.byref(opts),
+                                          fp._stream_ptr(stream)))
 
 
 class ExtractBatch:
@@ -70,21 +136,7 @@ class ExtractBatch:
         self._keep = []
         reqs = (NbExtractRequest * len(requests))()
         for i, r in enumerate(requests):
-            q = reqs[i]
-            arrays = [fp.as_nb_array(t, self._keep) for t in (r.volume, r.volume_weight, r.slice, r.slice_weight)]
-            self._keep.extend(a for a in arrays if a is not None)
-            q.volume = C.pointer(arrays[0])
-            q.volume_weight = C.pointer(arrays[1]) if arrays[1] is not None else None
-            q.slice = C.pointer(arrays[2])
-            q.slice_weight = C.pointer(arrays[3]) if arrays[3] is not None else None
-            for k in range(4):
-                q.volume_shape[k] = int(r.volume_shape[k])
-                q.slice_shape[k] = int(r.slice_shape[k])
-            sc = fp.as_nb_transform(r.inv_scaling, False, self._keep)
-            rot = fp.as_nb_transform(r.fwd_rotation, True, self._keep)
-            self._keep.extend([sc, rot])
-            q.inv_scaling = C.pointer(sc)
-            q.fwd_rotation = C.pointer(rot)
+            _fill_request(reqs[i], r, self._keep)
         self._keep.append(reqs)
         opts = fp._options(interp=interp, fftfreq_cutoff=fftfreq_cutoff, ews_radius=ews_radius,
                            w_windowed_sinc=w_windowed_sinc)

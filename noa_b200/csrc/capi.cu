@@ -7,7 +7,9 @@
 // constructors (FourierProject.hpp:199-231, 426-475, 577-609, 790-848), computed in float like the
 // reference's f32 coordinate type.
 #include "fp_args.cuh"
+#include "fp_pairs.cuh"
 
+#include "noa_b200/batch.h"
 #include "noa_b200/fourier_project.h"
 
 #include <cmath>
@@ -405,11 +407,66 @@ int finish_launch(cudaError_t err) { return finish(err); }
 
 int report_error(int code, const char* message) { return fail(code, "%s", message); }
 
+int check_pairs(const void* pairs, int64_t bytes, const ProjArgs& a, const char* name) {
+    const int64_t need = static_cast<int64_t>(a.vol_d) * a.vol_h * (a.vol_w / 2 + 1) * 16;
+    if (!pairs)
+        return fail(NB_ERROR_INVALID, "%s should not be NULL", name);
+    if (reinterpret_cast<uintptr_t>(pairs) % 16)
+        return fail(NB_ERROR_INVALID, "%s: the pair copy should be 16-byte aligned", name);
+    if (bytes < need)
+        return fail(NB_ERROR_INVALID, "%s: %lld bytes given, the pair copy needs %lld", name,
+                    static_cast<long long>(bytes), static_cast<long long>(need));
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(NB_ERROR_CUDA, "no CUDA device");
+    }
+    return check_device_pointer(pairs, name, device);
+}
+
 } // namespace nb
 
 using namespace nb;
 
 extern "C" {
+
+int64_t nb_volume_pairs_bytes(const int64_t volume_shape[4]) {
+    if (!volume_shape || volume_shape[1] <= 0 || volume_shape[2] <= 0 || volume_shape[3] <= 0)
+        return -1;
+    return volume_shape[1] * volume_shape[2] * (volume_shape[3] / 2 + 1) * 16;
+}
+
+int nb_volume_pairs(const nb_array* volume, const int64_t volume_shape[4], void* pairs, int64_t pairs_bytes,
+                    void* stream) {
+    if (!volume_shape)
+        return fail(NB_ERROR_INVALID, "volume_shape should not be NULL");
+    if (volume_shape[0] != 1)
+        return fail(NB_ERROR_INVALID, "the pair copy is made of one volume, got a batch of %lld",
+                    static_cast<long long>(volume_shape[0]));
+    if (!is_array(volume) || volume->dtype != NB_DTYPE_C32)
+        return fail(NB_ERROR_INVALID, "the pair copy needs a complex (c32) volume array");
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(NB_ERROR_CUDA, "no CUDA device");
+    }
+    int st = check_array(volume, volume_shape, "volume", false, device);
+    if (st != NB_OK)
+        return st;
+    ProjArgs a{};
+    a.in = make_src(volume, 1);
+    a.vol_d = static_cast<int>(volume_shape[1]);
+    a.vol_h = static_cast<int>(volume_shape[2]);
+    a.vol_w = static_cast<int>(volume_shape[3]);
+    a.in_cplx = 1;
+    a.interp = I_LINEAR;
+    a.wsize = 1;
+    if (!pairs_apply(a))
+        return fail(NB_ERROR_INVALID, "the pair copy must span fewer than 2^31 voxels");
+    if ((st = check_pairs(pairs, pairs_bytes, a, "pairs")) != NB_OK)
+        return st;
+    return finish(launch_make_pairs(a, static_cast<float4*>(pairs), static_cast<cudaStream_t>(stream)));
+}
 
 void nb_options_default(nb_options* o) {
     if (!o)

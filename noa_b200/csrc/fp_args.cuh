@@ -57,6 +57,8 @@ int prepare_extract(int32_t remap,
                     const nb_array* slice, const nb_array* slice_weight, const int64_t slice_shape[4],
                     const nb_transform* inv_scaling, const nb_transform* fwd_rotation,
                     const nb_options* options, ProjArgs& a);
+// Checks a caller's pair copy (nb_volume_pairs) of the volume of `a`: NB_OK or NB_ERROR_INVALID.
+int check_pairs(const void* pairs, int64_t bytes, const ProjArgs& a, const char* name);
 // NB_OK (clearing the thread's last error) or NB_ERROR_CUDA with the launch error's description.
 int finish_launch(cudaError_t err);
 // Sets the thread's last error and returns `code`.

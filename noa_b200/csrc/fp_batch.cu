@@ -13,6 +13,8 @@
 // cached per workload key in memory and in a small text file), and captures the launch — counter
 // reset + persistent kernel — into a CUDA graph. nb_extract_batch_run replays that graph on a stream.
 #include "fp_args.cuh"
+#include "fp_pairs.cuh"
+#include "fp_pool.cuh"
 #include "noa_b200/batch.h"
 
 #include <algorithm>
@@ -33,13 +35,54 @@ namespace {
 
 struct BatchReq {
     ProjArgs a;
+    const float4* pairs;      // pair copy of the volume (LINEAR fast path), or null
+    int ppt;                  // rows per thread: PAIRS_PPT with a pair copy, else 1
     int ntx;                  // tiles along u
     int tiles_per_slice;
     int64_t first_item;       // index of this request's first item
 };
+static_assert(sizeof(BatchReq) % 8 == 0, "BatchReq is staged in shared memory as 8-byte words");
+
+constexpr int PAIRS_PPT = 4;
 
 // One output pixel (b, y, u) of request `a`: the body of extract_kernel (fp_extract.cu), with 32-bit
 // volume offsets (batches require volumes addressable in 31 bits).
+// PAIRS_PPT output pixels (rows y0, y0 + dy, ...) of column u read through the volume's pair copy:
+// the body of extract_pairs_kernel (fp_extract.cu).
+template<bool OUT_C>
+__device__ __forceinline__ void extract_rows_pairs(const ProjArgs& a, const float4* pairs, int64_t b, int y0,
+                                                   int dy, int u) {
+    const Spectrum3 sp{a.vol_d, a.vol_h, a.vol_w, a.in_centered};
+    const int WP = a.vol_w / 2 + 1;
+    const float f1 = div(static_cast<float>(u), a.f_slice1);
+    float2 value[PAIRS_PPT];
+    bool inside[PAIRS_PPT];
+#pragma unroll
+    for (int r = 0; r < PAIRS_PPT; ++r) {
+        const int y = y0 + r * dy;
+        value[r] = make_float2(0.f, 0.f);
+        inside[r] = false;
+        if (y >= a.slice_h)
+            continue;
+        const float f0 = div(static_cast<float>(index2frequency(a.out_centered, y, a.slice_h)), a.f_slice0);
+        float fz, fy, fx;
+        slice2grid(f0, f1, a.scale, a.rot, b, a.ews, fz, fy, fx);
+        inside[r] = dot3(fz, fy, fx, fz, fy, fx) <= a.cutoff_sqd;
+        if (inside[r])
+            value[r] = to_output<true, OUT_C>(interp_linear_pairs(pairs, a.vol_h * WP, WP, sp, mul(fz, a.target0),
+                                                                  mul(fy, a.target1), mul(fx, a.target2)));
+    }
+#pragma unroll
+    for (int r = 0; r < PAIRS_PPT; ++r) {
+        const int y = y0 + r * dy;
+        if (y >= a.slice_h)
+            continue;
+        dst_store_stream<OUT_C>(a.out, b, y, u, value[r]);
+        if (a.out_w.present)
+            store_real_stream(a.out_w, b, y, u, inside[r] ? 1.f : 0.f);
+    }
+}
+
 template<int I, bool IN_C, bool OUT_C>
 __device__ __forceinline__ void extract_one(const ProjArgs& a, int64_t b, int y, int u) {
     const Spectrum3 sp{a.vol_d, a.vol_h, a.vol_w, a.in_centered};
@@ -90,22 +133,29 @@ constexpr int N_VARIANTS = 3;
 struct Variant { int ty, tx, wy, wx, min_ctas; };
 constexpr Variant VARIANTS[N_VARIANTS] = {{16, 16, 4, 8, 1}, {8, 32, 2, 16, 1}, {16, 16, 4, 8, 4}};
 
-template<int I, bool IN_C, bool OUT_C, int V>
-__global__ void __launch_bounds__(256, VARIANTS[V].min_ctas)
+// PAIRS_ONLY: every request reads a pair copy (LINEAR, complex); the generic path is compiled out so
+// the kernel fits 40 registers (6 CTAs per SM, like extract_pairs_kernel).
+template<int I, bool IN_C, bool OUT_C, int V, bool PAIRS_ONLY = false>
+__global__ void __launch_bounds__(256, PAIRS_ONLY ? 6 : VARIANTS[V].min_ctas)
 batch_extract_kernel(const BatchReq* __restrict__ reqs, int n_req, int64_t n_items,
                      unsigned long long* __restrict__ counter) {
     constexpr Variant VT = VARIANTS[V];
+    constexpr int WORDS = sizeof(BatchReq) / 8;
+    __shared__ unsigned long long s_req_words[WORDS];  // the current request, staged once per change
     __shared__ long long s_item;
     __shared__ int s_req;
+    const BatchReq& R = *reinterpret_cast<const BatchReq*>(s_req_words);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     constexpr int WARPS_X = VT.tx / VT.wx;
     const int ly = (warp / WARPS_X) * VT.wy + lane / VT.wx;
     const int lx = (warp % WARPS_X) * VT.wx + lane % VT.wx;
+    int staged = -1;   // request held in s_req_words
+    int found = 0;     // thread 0: request of the previous item (a CTA's items only increase)
     for (;;) {
         if (threadIdx.x == 0) {
             const long long item = static_cast<long long>(atomicAdd(counter, 1ull));
-            int lo = 0, hi = n_req - 1;
-            if (item < n_items) {
+            if (item < n_items && found + 1 < n_req && reqs[found + 1].first_item <= item) {
+                int lo = found + 1, hi = n_req - 1;
                 while (lo < hi) {
                     const int mid = (lo + hi + 1) / 2;
                     if (reqs[mid].first_item <= item)
@@ -113,24 +163,40 @@ batch_extract_kernel(const BatchReq* __restrict__ reqs, int n_req, int64_t n_ite
                     else
                         hi = mid - 1;
                 }
+                found = lo;
             }
             s_item = item;
-            s_req = lo;
+            s_req = found;
         }
         __syncthreads();
         const long long item = s_item;
         const int r = s_req;
-        __syncthreads();
         if (item >= n_items)
             break;
-        const BatchReq& R = reqs[r];
+        if (r != staged) {
+            const auto* src = reinterpret_cast<const unsigned long long*>(reqs + r);
+            for (int i = threadIdx.x; i < WORDS; i += blockDim.x)
+                s_req_words[i] = src[i];
+            staged = r;
+        }
+        __syncthreads();
         const int64_t local = item - R.first_item;
         const int64_t b = local / R.tiles_per_slice;
         const int tile = static_cast<int>(local - b * R.tiles_per_slice);
-        const int y = (tile / R.ntx) * VT.ty + ly;
         const int u = (tile % R.ntx) * VT.tx + lx;
-        if (y < R.a.slice_h && u < R.a.slice_w / 2 + 1)
-            extract_one<I, IN_C, OUT_C>(R.a, b, y, u);
+        if (u < R.a.slice_w / 2 + 1) {
+            if constexpr (I == I_LINEAR && IN_C) {
+                if (PAIRS_ONLY || R.pairs) {
+                    extract_rows_pairs<OUT_C>(R.a, R.pairs, b, (tile / R.ntx) * (VT.ty * PAIRS_PPT) + ly, VT.ty, u);
+                    continue;
+                }
+            }
+            if constexpr (!PAIRS_ONLY) {
+                const int y = (tile / R.ntx) * VT.ty + ly;
+                if (y < R.a.slice_h)
+                    extract_one<I, IN_C, OUT_C>(R.a, b, y, u);
+            }
+        }
     }
 }
 
@@ -259,17 +325,23 @@ int max_blocks_per_sm(KernelFn fn) {
     return n > 0 ? n : 1;
 }
 
+// Tile fields of one request for a variant; `first` is its first item and advances past its items.
+void set_tiles(BatchReq& r, const Variant& vt, int64_t& first) {
+    r.ppt = r.pairs ? PAIRS_PPT : 1;
+    const int wp = r.a.slice_w / 2 + 1;
+    const int th = vt.ty * r.ppt;
+    r.ntx = (wp + vt.tx - 1) / vt.tx;
+    r.tiles_per_slice = r.ntx * ((r.a.slice_h + th - 1) / th);
+    r.first_item = first;
+    first += static_cast<int64_t>(r.tiles_per_slice) * r.a.n_slices;
+}
+
 // Fills the per-variant tile fields and uploads the descriptors.
 cudaError_t upload(nb_extract_batch_t* h, int variant, cudaStream_t stream) {
     const Variant vt = VARIANTS[variant];
     int64_t first = 0;
-    for (BatchReq& r : h->host_reqs) {
-        const int wp = r.a.slice_w / 2 + 1;
-        r.ntx = (wp + vt.tx - 1) / vt.tx;
-        r.tiles_per_slice = r.ntx * ((r.a.slice_h + vt.ty - 1) / vt.ty);
-        r.first_item = first;
-        first += static_cast<int64_t>(r.tiles_per_slice) * r.a.n_slices;
-    }
+    for (BatchReq& r : h->host_reqs)
+        set_tiles(r, vt, first);
     h->n_items = first;
     cudaError_t err = cudaMemcpyAsync(h->d_reqs, h->host_reqs.data(), h->host_reqs.size() * sizeof(BatchReq),
                                       cudaMemcpyHostToDevice, stream);
@@ -346,6 +418,34 @@ void release(nb_extract_batch_t* h) {
     delete h;
 }
 
+// Stages the descriptors of `h` in stream-ordered device memory and launches `fn` once on `s`.
+int launch_once(nb_extract_batch_t& h, KernelFn fn, int variant, int blocks_per_sm, cudaStream_t s) {
+    const Variant vt = VARIANTS[variant];
+    int64_t first = 0;
+    for (BatchReq& r : h.host_reqs)
+        set_tiles(r, vt, first);
+    if (first == 0)
+        return finish_launch(cudaSuccess);
+    // Descriptors then the work counter, in one stream-ordered allocation.
+    const size_t desc_bytes = (h.host_reqs.size() * sizeof(BatchReq) + 255) / 256 * 256;
+    void* dev = scratch_alloc(desc_bytes + sizeof(unsigned long long), s);
+    if (!dev)
+        return report_error(NB_ERROR_OOM, "cannot allocate the batch descriptors");
+    auto* d_reqs = static_cast<BatchReq*>(dev);
+    auto* d_counter = reinterpret_cast<unsigned long long*>(static_cast<char*>(dev) + desc_bytes);
+    // Pageable source: the runtime stages it before returning, so the host vector may go right after.
+    cudaError_t err = cudaMemcpyAsync(d_reqs, h.host_reqs.data(), h.host_reqs.size() * sizeof(BatchReq),
+                                      cudaMemcpyHostToDevice, s);
+    if (err == cudaSuccess)
+        err = cudaMemsetAsync(d_counter, 0, sizeof(unsigned long long), s);
+    if (err == cudaSuccess) {
+        fn<<<sm_count() * blocks_per_sm, 256, 0, s>>>(d_reqs, static_cast<int>(h.host_reqs.size()), first, d_counter);
+        err = cudaGetLastError();
+    }
+    scratch_free(dev, s);
+    return finish_launch(err);
+}
+
 } // namespace
 } // namespace nb
 
@@ -386,6 +486,7 @@ int nb_extract_batch_create(int32_t remap, const nb_extract_request* requests, i
             return report_error(NB_ERROR_INVALID, "all requests of a batch must have the same value types");
         }
         h->host_reqs[static_cast<size_t>(i)].a = a;
+        h->host_reqs[static_cast<size_t>(i)].pairs = nullptr;
     }
     if (cudaMalloc(&h->d_reqs, h->host_reqs.size() * sizeof(BatchReq)) != cudaSuccess ||
         cudaMalloc(&h->d_counter, sizeof(unsigned long long)) != cudaSuccess) {
@@ -484,6 +585,64 @@ int nb_extract_batch_info(nb_extract_batch batch, nb_batch_info* info) {
 int nb_extract_batch_destroy(nb_extract_batch batch) {
     release(batch);
     return NB_OK;
+}
+
+int nb_extract_batch_launch(int32_t remap, const nb_extract_request_ex* requests, int64_t n_requests,
+                            const nb_options* options, void* stream) {
+    if (!requests || n_requests <= 0)
+        return report_error(NB_ERROR_INVALID, "a batch needs at least one request");
+    if (n_requests > (int64_t(1) << 30))
+        return report_error(NB_ERROR_INVALID, "too many requests");
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    nb_extract_batch_t h;  // host-side description only: no graph, no device descriptors of its own
+    h.host_reqs.resize(static_cast<size_t>(n_requests));
+    for (int64_t i = 0; i < n_requests; ++i) {
+        const nb_extract_request& q = requests[i].call;
+        ProjArgs a{};
+        int st = prepare_extract(remap, q.volume, q.volume_weight, q.volume_shape, q.slice, q.slice_weight,
+                                 q.slice_shape, q.inv_scaling, q.fwd_rotation, options, a);
+        if (st != NB_OK)
+            return st;
+        if (a.wide_in)
+            return report_error(NB_ERROR_INVALID, "batched volumes must span fewer than 2^31 elements");
+        if (i == 0) {
+            h.interp = a.interp;
+            h.in_cplx = a.in_cplx;
+            h.out_cplx = a.out_cplx;
+        } else if (a.in_cplx != h.in_cplx || a.out_cplx != h.out_cplx) {
+            return report_error(NB_ERROR_INVALID, "all requests of a batch must have the same value types");
+        }
+        BatchReq& r = h.host_reqs[static_cast<size_t>(i)];
+        r.a = a;
+        r.pairs = nullptr;
+        if (requests[i].volume_pairs && pairs_apply(a)) {
+            if ((st = check_pairs(requests[i].volume_pairs, requests[i].volume_pairs_bytes, a, "volume_pairs")) != NB_OK)
+                return st;
+            r.pairs = static_cast<const float4*>(requests[i].volume_pairs);
+        }
+    }
+    bool all_pairs = true;
+    for (const BatchReq& r : h.host_reqs)
+        all_pairs = all_pairs && r.pairs != nullptr;
+    h.key = workload_key(&h);
+    Config cfg{0, 0};
+    if (all_pairs) {
+        // Pair copies everywhere: the lean pairs-only kernel, tile 64 x 16, full occupancy.
+        const KernelFn fn = h.out_cplx ? batch_extract_kernel<I_LINEAR, true, true, 0, true>
+                                       : batch_extract_kernel<I_LINEAR, true, false, 0, true>;
+        return launch_once(h, fn, 0, max_blocks_per_sm(fn), s);
+    }
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        load_cache_locked();
+        auto it = g_tuned.find(h.key);
+        if (it != g_tuned.end())
+            cfg = {it->second.first, it->second.second};
+    }
+    if (cfg.blocks_per_sm <= 0)
+        cfg.blocks_per_sm = max_blocks_per_sm(pick_kernel(h.interp, h.in_cplx, h.out_cplx, cfg.variant));
+    return launch_once(h, pick_kernel(h.interp, h.in_cplx, h.out_cplx, cfg.variant), cfg.variant,
+                       cfg.blocks_per_sm, s);
 }
 
 } // extern "C"

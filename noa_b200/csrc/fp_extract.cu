@@ -11,6 +11,7 @@
 // the w offsets of the z-shifted samples — but sums in registers, in w order, instead of zeroing the
 // outputs and adding atomically, so it is deterministic and needs no extra pass.
 #include "fp_args.cuh"
+#include "fp_pairs.cuh"
 #include "fp_pool.cuh"
 
 namespace nb {
@@ -19,13 +20,8 @@ namespace {
 constexpr int TY = 16, TX = 16, EXTRACT_THREADS = TY * TX;
 
 // ---------------------------------------------------------------------------------------------------
-// Fast LINEAR path over a pair copy of the volume.
-//
-// The copy is dense (D x H x W/2+1) and element (z, y, x) holds the two x-neighbours v[z][y][x] and
-// v[z][y][x+1] (zero past the last column) as one float4, so the 2x2x2 trilinear cell is 4 aligned
-// 16-byte loads instead of 8 scattered 8-byte ones. Each thread interpolates PAIR_PPT pixels (rows
-// y, y+16, ...) of one column, keeping more loads in flight. The taps, weights and summation order
-// are those of interp_linear_3d, so the results are bit-identical to the generic path.
+// Fast LINEAR path over a pair copy of the volume (fp_pairs.cuh). Each thread interpolates PAIR_PPT
+// pixels (rows y, y+16, ...) of one column, keeping more loads in flight.
 // ---------------------------------------------------------------------------------------------------
 constexpr int PAIR_PPT = 4;
 
@@ -43,50 +39,6 @@ __global__ void make_pairs(const __grid_constant__ ProjArgs a, float4* __restric
         const float2 v1 = x + 1 < WP ? vol[off + a.in.s2] : make_float2(0.f, 0.f);
         pairs[i] = make_float4(v0.x, v0.y, v1.x, v1.y);
     }
-}
-
-__device__ __forceinline__ float2 interp_linear_pairs(const float4* __restrict__ pairs, int sz, int sy,
-                                                      const Spectrum3& sp, float q0, float q1, float q2) {
-    float conjugate = 1.f;
-    if (q2 < 0.f) {
-        q0 = -q0; q1 = -q1; q2 = -q2;
-        conjugate = -1.f;
-    }
-    const float fl0 = floorf(q0), fl1 = floorf(q1), fl2 = floorf(q2);
-    const int b0 = static_cast<int>(fl0), b1 = static_cast<int>(fl1), b2 = static_cast<int>(fl2);
-    const float t0 = sub(q0, fl0), t1 = sub(q1, fl1), t2 = sub(q2, fl2);
-    const float w0[2] = {sub(1.f, t0), t0};
-    const float w1[2] = {sub(1.f, t1), t1};
-    const float w20 = sub(1.f, t2);
-    const int lo0 = -sp.n0 / 2, hi0 = (sp.n0 - 1) / 2;
-    const int lo1 = -sp.n1 / 2, hi1 = (sp.n1 - 1) / 2;
-    const int hi2 = sp.n2 / 2;
-    const bool okx0 = b2 >= 0 && b2 <= hi2;
-    const bool okx1 = b2 + 1 >= 0 && b2 + 1 <= hi2;
-    float2 value = make_float2(0.f, 0.f);
-#pragma unroll
-    for (int z = 0; z < 2; ++z) {
-        const int iz = b0 + z;
-        const bool okz = iz >= lo0 && iz <= hi0;
-        const int oz = frequency2index(sp.centered, iz, sp.n0) * sz;
-        float2 vz = make_float2(0.f, 0.f);
-#pragma unroll
-        for (int y = 0; y < 2; ++y) {
-            const int iy = b1 + y;
-            const bool oky = iy >= lo1 && iy <= hi1;
-            float2 vy = make_float2(0.f, 0.f);
-            if (okz && oky && okx0) {
-                const float4 p = __ldg(pairs + (oz + frequency2index(sp.centered, iy, sp.n1) * sy + b2));
-                vy = cfma(make_float2(p.x, p.y), w20, vy);
-                if (okx1)
-                    vy = cfma(make_float2(p.z, p.w), t2, vy);
-            }
-            vz = cfma(vy, w1[y], vz);
-        }
-        value = cfma(vz, w0[z], value);
-    }
-    value.y *= conjugate;
-    return value;
 }
 
 template<bool OUT_C>
@@ -133,14 +85,12 @@ extract_pairs_kernel(const __grid_constant__ ProjArgs a, const float4* __restric
     }
 }
 
-// Whether the pair path applies: LINEAR, complex volume, no input weights, no EWS, no scaling, no
-// w-window, a dense copy addressable in 32 bits, and enough pixels to amortise the copy.
+// Whether the per-call pair path applies: the pair copy is readable (pairs_apply) and there are enough
+// pixels to amortise making it.
 bool use_pairs(const ProjArgs& a) {
-    const int64_t wp_vol = a.vol_w / 2 + 1;
-    const int64_t vox = static_cast<int64_t>(a.vol_d) * a.vol_h * wp_vol;
+    const int64_t vox = static_cast<int64_t>(a.vol_d) * a.vol_h * (a.vol_w / 2 + 1);
     const int64_t pix = a.n_slices * a.slice_h * static_cast<int64_t>(a.slice_w / 2 + 1);
-    return a.interp == I_LINEAR && a.in_cplx && !a.in_w.present && !a.in.is_value && !a.ews.on &&
-           a.scale.kind == 0 && a.wsize <= 1 && vox < (int64_t(1) << 31) && pix >= 2 * vox;
+    return pairs_apply(a) && pix >= 2 * vox;
 }
 
 cudaError_t launch_pairs(const ProjArgs& a, cudaStream_t stream, bool& done) {
@@ -150,10 +100,7 @@ cudaError_t launch_pairs(const ProjArgs& a, cudaStream_t stream, bool& done) {
     float4* pairs = static_cast<float4*>(scratch_alloc(static_cast<size_t>(vox) * sizeof(float4), stream));
     if (!pairs)
         return cudaSuccess; // no scratch: the caller takes the generic path
-    const int threads = 256;
-    const int64_t blocks = (vox + threads - 1) / threads;
-    const int grid_c = static_cast<int>(blocks < static_cast<int64_t>(sm_count()) * 16 ? blocks : sm_count() * 16);
-    make_pairs<<<grid_c, threads, 0, stream>>>(a, pairs);
+    launch_make_pairs(a, pairs, stream);
     const int wp = a.slice_w / 2 + 1;
     const int ntx = (wp + TX - 1) / TX, nty = (a.slice_h + TY * PAIR_PPT - 1) / (TY * PAIR_PPT);
     const dim3 grid(static_cast<unsigned>(ntx * nty), static_cast<unsigned>(a.n_slices < 65535 ? a.n_slices : 65535));
@@ -245,6 +192,16 @@ cudaError_t launch_interp(const ProjArgs& a, cudaStream_t stream) {
 }
 
 } // namespace
+
+cudaError_t launch_make_pairs(const ProjArgs& a, float4* pairs, cudaStream_t stream) {
+    const int64_t vox = static_cast<int64_t>(a.vol_d) * a.vol_h * (a.vol_w / 2 + 1);
+    const int threads = 256;
+    const int64_t blocks = (vox + threads - 1) / threads;
+    const int grid = static_cast<int>(blocks < static_cast<int64_t>(sm_count()) * 16 ? blocks : sm_count() * 16);
+    if (grid > 0)
+        make_pairs<<<grid, threads, 0, stream>>>(a, pairs);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_extract(const ProjArgs& a, cudaStream_t stream) {
     if (a.n_slices > 0 && use_pairs(a)) {
