@@ -152,6 +152,7 @@ def run_gpu(args) -> None:
     import torch
     import torch.distributed as dist
     from noa_b200 import fourier_project as fp
+    from noa_b200 import shard
 
     world, rank, local = dist_setup()
     vol, slices_in, rot_e, rot_i = make_inputs(seed=1000 * rank)
@@ -197,12 +198,9 @@ def run_gpu(args) -> None:
     step_ms = sum(t_ext + t_ras) / args.steps
     ext_ms, ras_ms = statistics.mean(t_ext), statistics.mean(t_ras)
     if world > 1:
-        t = torch.tensor([step_ms, ext_ms, ras_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        step_ms, ext_ms, ras_ms = t.tolist()
+        step_ms, ext_ms, ras_ms = shard.max_over_ranks([step_ms, ext_ms, ras_ms], device="cuda")
         # The reconstruction's one exchange: sum the per-rank partial grids (after the timed region).
-        dist.all_reduce(grid)
-        dist.all_reduce(grid_w)
+        shard.allreduce_grids(grid, grid_w)
         torch.cuda.synchronize()
 
     # End to end through the public API with host buffers: H2D of the step's inputs (volume,
@@ -235,9 +233,7 @@ def run_gpu(args) -> None:
             e2e_ms.append(s0.elapsed_time(s1))
     e2e = statistics.mean(e2e_ms)
     if world > 1:
-        t = torch.tensor([e2e], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e = t.item()
+        e2e = shard.max_over_ranks([e2e], device="cuda")[0]
 
     if rank == 0:
         ab = algorithmic_bytes(N, SLICES)
