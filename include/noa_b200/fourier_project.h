@@ -108,6 +108,20 @@ NB_API int nb_insert_central_slices_3d(
     const nb_transform* fwd_scaling, const nb_transform* inv_rotation,
     const nb_options* options, void* stream);
 
+/* Slice-major scatter form of nb_insert_central_slices_3d (no counterpart in the reference): the same
+ * per-(voxel, slice) terms — same windowed sinc, same 2-D interpolation, same cutoff — but each slice
+ * visits the voxels of its slab |fz| <= fftfreq_blackman and adds its terms with atomics, so the sum
+ * over slices is in an unspecified order (results match the gather form to float rounding, not
+ * bit-exactly). Needs a dense accumulator of the volume (16 bytes per rfft voxel with weights) from the
+ * library's stream-ordered pool; with an Ewald-sphere curvature, or without that memory, it runs the
+ * gather form. Same arguments and errors as nb_insert_central_slices_3d. */
+NB_API int nb_insert_central_slices_3d_scatter(
+    int32_t remap,
+    const nb_array* slice, const nb_array* slice_weight, const int64_t slice_shape[4],
+    const nb_array* volume, const nb_array* volume_weight, const int64_t volume_shape[4],
+    const nb_transform* fwd_scaling, const nb_transform* inv_rotation,
+    const nb_options* options, void* stream);
+
 /* extract_central_slices_3d: 3-D spectrum interpolation at every pixel of every output slice (=). */
 NB_API int nb_extract_central_slices_3d(
     int32_t remap,

@@ -403,6 +403,52 @@ int prepare_extract(
     return NB_OK;
 }
 
+int prepare_insert(
+    int32_t remap,
+    const nb_array* slice, const nb_array* slice_weight, const int64_t slice_shape[4],
+    const nb_array* volume, const nb_array* volume_weight, const int64_t volume_shape[4],
+    const nb_transform* fwd_scaling, const nb_transform* inv_rotation,
+    const nb_options* options, ProjArgs& a) {
+    int device = 0;
+    int st = common_checks(Op::INSERT, remap, slice, slice_weight, slice_shape,
+                           volume, volume_weight, volume_shape, options, device);
+    if (st != NB_OK) return st;
+    if ((st = check_transform(fwd_scaling, slice_shape[0], false, "fwd_scaling", device)) != NB_OK) return st;
+    if ((st = check_transform(inv_rotation, slice_shape[0], true, "inv_rotation", device)) != NB_OK) return st;
+
+    a = ProjArgs{};
+    a.in = make_src(slice, 0);
+    a.in_w = make_src(slice_weight, 0);
+    a.out = make_dst(volume, 1);
+    a.out_w = make_dst(volume_weight, 1);
+    a.scale = make_xform(fwd_scaling);
+    a.rot = make_xform(inv_rotation);
+    a.ews = make_ews(options->ews_radius);
+    a.n_slices = slice_shape[0];
+    a.slice_h = static_cast<int>(slice_shape[2]);
+    a.slice_w = static_cast<int>(slice_shape[3]);
+    a.vol_d = static_cast<int>(volume_shape[1]);
+    a.vol_h = static_cast<int>(volume_shape[2]);
+    a.vol_w = static_cast<int>(volume_shape[3]);
+    a.in_centered = (remap & 4) != 0;
+    a.out_centered = (remap & 8) != 0;
+    a.interp = interp_family(options->interp);
+    a.f_slice0 = static_cast<float>(slice_shape[2]);
+    a.f_slice1 = static_cast<float>(slice_shape[3]);
+    float t[3];
+    target3(options, volume_shape, t);
+    a.target0 = t[0]; a.target1 = t[1]; a.target2 = t[2];
+    a.cutoff_sqd = cutoff_sqd(options);
+    float tmin = t[0];
+    if (t[1] < tmin) tmin = t[1];
+    if (t[2] < tmin) tmin = t[2];
+    a.fs = fmax_ref(static_cast<float>(options->fftfreq_sinc), 1.f / tmin);
+    a.fb = fmax_ref(static_cast<float>(options->fftfreq_blackman), 1.f / tmin);
+    a.in_cplx = is_complex(slice->dtype);
+    a.out_cplx = is_complex(volume->dtype);
+    return NB_OK;
+}
+
 int finish_launch(cudaError_t err) { return finish(err); }
 
 int report_error(int code, const char* message) { return fail(code, "%s", message); }
@@ -503,44 +549,24 @@ int nb_insert_central_slices_3d(
     const nb_array* volume, const nb_array* volume_weight, const int64_t volume_shape[4],
     const nb_transform* fwd_scaling, const nb_transform* inv_rotation,
     const nb_options* options, void* stream) {
-    int device = 0;
-    int st = common_checks(Op::INSERT, remap, slice, slice_weight, slice_shape,
-                           volume, volume_weight, volume_shape, options, device);
-    if (st != NB_OK) return st;
-    if ((st = check_transform(fwd_scaling, slice_shape[0], false, "fwd_scaling", device)) != NB_OK) return st;
-    if ((st = check_transform(inv_rotation, slice_shape[0], true, "inv_rotation", device)) != NB_OK) return st;
-
     ProjArgs a{};
-    a.in = make_src(slice, 0);
-    a.in_w = make_src(slice_weight, 0);
-    a.out = make_dst(volume, 1);
-    a.out_w = make_dst(volume_weight, 1);
-    a.scale = make_xform(fwd_scaling);
-    a.rot = make_xform(inv_rotation);
-    a.ews = make_ews(options->ews_radius);
-    a.n_slices = slice_shape[0];
-    a.slice_h = static_cast<int>(slice_shape[2]);
-    a.slice_w = static_cast<int>(slice_shape[3]);
-    a.vol_d = static_cast<int>(volume_shape[1]);
-    a.vol_h = static_cast<int>(volume_shape[2]);
-    a.vol_w = static_cast<int>(volume_shape[3]);
-    a.in_centered = (remap & 4) != 0;
-    a.out_centered = (remap & 8) != 0;
-    a.interp = interp_family(options->interp);
-    a.f_slice0 = static_cast<float>(slice_shape[2]);
-    a.f_slice1 = static_cast<float>(slice_shape[3]);
-    float t[3];
-    target3(options, volume_shape, t);
-    a.target0 = t[0]; a.target1 = t[1]; a.target2 = t[2];
-    a.cutoff_sqd = cutoff_sqd(options);
-    float tmin = t[0];
-    if (t[1] < tmin) tmin = t[1];
-    if (t[2] < tmin) tmin = t[2];
-    a.fs = fmax_ref(static_cast<float>(options->fftfreq_sinc), 1.f / tmin);
-    a.fb = fmax_ref(static_cast<float>(options->fftfreq_blackman), 1.f / tmin);
-    a.in_cplx = is_complex(slice->dtype);
-    a.out_cplx = is_complex(volume->dtype);
+    const int st = prepare_insert(remap, slice, slice_weight, slice_shape, volume, volume_weight, volume_shape,
+                                  fwd_scaling, inv_rotation, options, a);
+    if (st != NB_OK) return st;
     return finish(launch_insert(a, static_cast<cudaStream_t>(stream)));
+}
+
+int nb_insert_central_slices_3d_scatter(
+    int32_t remap,
+    const nb_array* slice, const nb_array* slice_weight, const int64_t slice_shape[4],
+    const nb_array* volume, const nb_array* volume_weight, const int64_t volume_shape[4],
+    const nb_transform* fwd_scaling, const nb_transform* inv_rotation,
+    const nb_options* options, void* stream) {
+    ProjArgs a{};
+    const int st = prepare_insert(remap, slice, slice_weight, slice_shape, volume, volume_weight, volume_shape,
+                                  fwd_scaling, inv_rotation, options, a);
+    if (st != NB_OK) return st;
+    return finish(launch_insert_scatter(a, static_cast<cudaStream_t>(stream)));
 }
 
 int nb_extract_central_slices_3d(

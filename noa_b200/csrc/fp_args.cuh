@@ -43,6 +43,7 @@ cudaError_t launch_extract(const ProjArgs& a, cudaStream_t stream);
 cudaError_t launch_rasterize(const ProjArgs& a, cudaStream_t stream);
 cudaError_t launch_insert(const ProjArgs& a, cudaStream_t stream);
 cudaError_t launch_insert_extract(const ProjArgs& a, cudaStream_t stream);
+cudaError_t launch_insert_scatter(const ProjArgs& a, cudaStream_t stream);
 
 // Argument checks and per-call constants of nb_rasterize_central_slices_3d (capi.cu); fills `a` and
 // returns NB_OK, or an NB_ERROR_* code with the thread's last-error message set.
@@ -51,6 +52,12 @@ int prepare_rasterize(int32_t remap,
                       const nb_array* volume, const nb_array* volume_weight, const int64_t volume_shape[4],
                       const nb_transform* inv_scaling, const nb_transform* fwd_rotation,
                       const nb_options* options, ProjArgs& a);
+// Same for nb_insert_central_slices_3d (and its scatter form).
+int prepare_insert(int32_t remap,
+                   const nb_array* slice, const nb_array* slice_weight, const int64_t slice_shape[4],
+                   const nb_array* volume, const nb_array* volume_weight, const int64_t volume_shape[4],
+                   const nb_transform* fwd_scaling, const nb_transform* inv_rotation,
+                   const nb_options* options, ProjArgs& a);
 // Same for nb_extract_central_slices_3d.
 int prepare_extract(int32_t remap,
                     const nb_array* volume, const nb_array* volume_weight, const int64_t volume_shape[4],

@@ -159,6 +159,21 @@ __device__ __forceinline__ void slice2grid(float f0, float f1, const XformView& 
     rotate(rot, batch, z, y, x);
 }
 
+// Row 0 of the (inverse) rotation of slice i, so that grid2slice's fz = row . f.
+__device__ __forceinline__ float3 rotation_row0(const XformView& r, int64_t i) {
+    if (r.kind == 3) {
+        float a0 = 1.f, a1 = 0.f, a2 = 0.f;
+        float b0 = 0.f, b1 = 1.f, b2 = 0.f;
+        float c0 = 0.f, c1 = 0.f, c2 = 1.f;
+        rotate(r, i, a0, a1, a2);
+        rotate(r, i, b0, b1, b2);
+        rotate(r, i, c0, c1, c2);
+        return make_float3(a0, b0, c0);
+    }
+    const float* m = xform_ptr(r, i, 12);
+    return make_float3(m[0], m[1], m[2]);
+}
+
 // fourier_grid2slice (FourierProject.hpp:71-95): returns fz, and the 2-D frequency in (f0, f1).
 __device__ __forceinline__ float grid2slice(float z, float y, float x, const XformView& scale,
                                             const XformView& rot, int64_t batch, const Ews& ews,

@@ -17,21 +17,6 @@ namespace {
 constexpr int BZ = 4, BY = 8, BX = 8;
 constexpr int INSERT_THREADS = BZ * BY * BX;
 
-// Row 0 of the inverse rotation of slice i: fz = row . f.
-__device__ __forceinline__ float3 rotation_row0(const XformView& r, int64_t i) {
-    if (r.kind == 3) {
-        float a0 = 1.f, a1 = 0.f, a2 = 0.f;
-        float b0 = 0.f, b1 = 1.f, b2 = 0.f;
-        float c0 = 0.f, c1 = 0.f, c2 = 1.f;
-        rotate(r, i, a0, a1, a2);
-        rotate(r, i, b0, b1, b2);
-        rotate(r, i, c0, c1, c2);
-        return make_float3(a0, b0, c0);
-    }
-    const float* m = xform_ptr(r, i, 12);
-    return make_float3(m[0], m[1], m[2]);
-}
-
 template<int I, bool IN_C, bool OUT_C>
 __global__ void __launch_bounds__(INSERT_THREADS)
 insert_kernel(const __grid_constant__ ProjArgs a, int nbz, int nby, int nbx) {

@@ -73,11 +73,13 @@ def lib() -> C.CDLL:
         h.nb_rasterize_central_slices_3d_static_scratch.argtypes = [C.c_int32, arr, arr, shape, arr, arr, shape, xf, xf,
                                                                    opt, C.c_void_p]
         h.nb_insert_central_slices_3d.argtypes = [C.c_int32, arr, arr, shape, arr, arr, shape, xf, xf, opt, C.c_void_p]
+        h.nb_insert_central_slices_3d_scatter.argtypes = [C.c_int32, arr, arr, shape, arr, arr, shape, xf, xf, opt,
+                                                          C.c_void_p]
         h.nb_extract_central_slices_3d.argtypes = [C.c_int32, arr, arr, shape, arr, arr, shape, xf, xf, opt, C.c_void_p]
         h.nb_insert_and_extract_central_slices_3d.argtypes = [C.c_int32, arr, arr, shape, arr, arr, shape,
                                                                xf, xf, xf, xf, opt, C.c_void_p]
         for f in ("nb_rasterize_central_slices_3d", "nb_rasterize_central_slices_3d_static_scratch",
-                  "nb_insert_central_slices_3d",
+                  "nb_insert_central_slices_3d", "nb_insert_central_slices_3d_scatter",
                   "nb_extract_central_slices_3d", "nb_insert_and_extract_central_slices_3d"):
             getattr(h, f).restype = C.c_int
         h.nb_last_error.restype = C.c_char_p
@@ -274,6 +276,22 @@ def insert_central_slices_3d(remap: str, slice, slice_weight, slice_shape, volum
     o = _options(interp=interp, fftfreq_cutoff=fftfreq_cutoff, target_shape=target_shape,
                  ews_radius=ews_radius, windowed_sinc=windowed_sinc)
     _check(lib().nb_insert_central_slices_3d(
+        REMAPS[remap], _ref(as_nb_array(slice, keep)), _ref(as_nb_array(slice_weight, keep)), _shape(slice_shape),
+        _ref(as_nb_array(volume, keep)), _ref(as_nb_array(volume_weight, keep)), _shape(volume_shape),
+        _ref(as_nb_transform(fwd_scaling, False, keep)), _ref(as_nb_transform(inv_rotation, True, keep)),
+        C.byref(o), _stream_ptr(stream)))
+
+
+def insert_central_slices_3d_scatter(remap: str, slice, slice_weight, slice_shape, volume, volume_weight,
+                                     volume_shape, fwd_scaling, inv_rotation, *, interp="linear",
+                                     windowed_sinc=None, fftfreq_cutoff=0.5, target_shape=None,
+                                     ews_radius=(0.0, 0.0), stream=None) -> None:
+    """Slice-major atomic scatter form of ``insert_central_slices_3d``: the same terms, summed over the
+    slices in an unspecified order (no counterpart in the reference; see fourier_project.h)."""
+    keep = []
+    o = _options(interp=interp, fftfreq_cutoff=fftfreq_cutoff, target_shape=target_shape,
+                 ews_radius=ews_radius, windowed_sinc=windowed_sinc)
+    _check(lib().nb_insert_central_slices_3d_scatter(
         REMAPS[remap], _ref(as_nb_array(slice, keep)), _ref(as_nb_array(slice_weight, keep)), _shape(slice_shape),
         _ref(as_nb_array(volume, keep)), _ref(as_nb_array(volume_weight, keep)), _shape(volume_shape),
         _ref(as_nb_transform(fwd_scaling, False, keep)), _ref(as_nb_transform(inv_rotation, True, keep)),

@@ -101,12 +101,12 @@ def _device_volume(n: int, gen, device):
     return (torch.complex(re, im) * (amp * (0.5 ** 0.5)))[None].contiguous()
 
 
-def _device_slices(count: int, n: int, gen, device, bfactor: float = 100.0):
-    """synthetic.make_slices's distribution (non-centered layout), drawn on the device."""
+def _device_slices(count: int, n: int, gen, device, bfactor: float = 100.0, centered: bool = False):
+    """synthetic.make_slices's distribution, drawn on the device (non-centered or centered layout)."""
     import torch
     wp = n // 2 + 1
     i = torch.arange(n, device=device)
-    fy = torch.where(i < (n + 1) // 2, i, i - n).to(torch.float32) / n
+    fy = (i - n // 2 if centered else torch.where(i < (n + 1) // 2, i, i - n)).to(torch.float32) / n
     fx = torch.arange(wp, device=device, dtype=torch.float32) / n
     env = torch.exp(-bfactor * (fy[:, None] ** 2 + fx[None, :] ** 2) / 4)
     out = torch.empty((count, 1, n, wp), dtype=torch.complex64, device=device)

@@ -22,8 +22,9 @@ def _xform(a):
     return torch.from_numpy(np.ascontiguousarray(a)).cuda()
 
 
-def run(call: Call, stream=None):
-    """Copies the call's inputs to the device, runs the CUDA path, returns (out, out_w) as numpy."""
+def run(call: Call, stream=None, scatter=False):
+    """Copies the call's inputs to the device, runs the CUDA path, returns (out, out_w) as numpy.
+    ``scatter``: insertions run the slice-major scatter form instead of the gather form."""
     inp = call.inp_value if call.inp_value is not None else _dev(call.inp)
     inp_w = _dev(call.inp_w)
     out = _dev(call.out)
@@ -38,9 +39,9 @@ def run(call: Call, stream=None):
                                        scale, rot, fftfreq_cutoff=call.cutoff, target_shape=target,
                                        ews_radius=call.ews, stream=stream)
     elif call.func == "insert":
-        fp.insert_central_slices_3d(call.remap, inp, inp_w, call.in_shape, out, out_w, call.out_shape,
-                                    scale, rot, interp=interp, windowed_sinc=ws, fftfreq_cutoff=call.cutoff,
-                                    target_shape=target, ews_radius=call.ews, stream=stream)
+        f = fp.insert_central_slices_3d_scatter if scatter else fp.insert_central_slices_3d
+        f(call.remap, inp, inp_w, call.in_shape, out, out_w, call.out_shape, scale, rot, interp=interp,
+          windowed_sinc=ws, fftfreq_cutoff=call.cutoff, target_shape=target, ews_radius=call.ews, stream=stream)
     elif call.func == "extract":
         fp.extract_central_slices_3d(call.remap, inp, inp_w, call.in_shape, out, out_w, call.out_shape,
                                      scale, rot, interp=interp, w_windowed_sinc=wws, fftfreq_cutoff=call.cutoff,

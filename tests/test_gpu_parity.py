@@ -46,6 +46,28 @@ def test_gpu_matches_oracle(case):
         assert errw <= tol, f"weights rel L2 {errw:.3e} > {tol:g}"
 
 
+def _insert_cases():
+    return [c for c in _gpu_cases() if c["func"] == "insert"] + [
+        default_case("insert", n=40, nslices=60, out_w=True, sinc=(-1.0, 6 / 40), remap="hc2hc", seed=620),
+        default_case("insert", n=33, nslices=30, out_w=True, in_w=True, sinc=(0.03, 0.1), remap="h2hc", seed=621),
+        default_case("insert", n=32, nslices=20, in_dt="c32", out_dt="f32", sinc=(-1.0, 0.1), seed=622),
+    ]
+
+
+@pytest.mark.parametrize("case", _insert_cases(), ids=case_id)
+def test_gpu_scatter_insert_matches_oracle(case):
+    """The slice-major scatter form: the gather form's terms, summed in atomic order (tolerance 1e-5)."""
+    import gpu_run
+    call = build(case)
+    ref = clone(call)
+    assert FpOracle().run(ref, 8) == 0
+    out, out_w = gpu_run.run(clone(call), scatter=True)
+    err = rel_l2(out, ref.out)
+    assert err <= TOL["insert"], f"rel L2 {err:.3e}"
+    if ref.out_w is not None:
+        assert rel_l2(out_w, ref.out_w) <= TOL["insert"]
+
+
 def test_gpu_rejects_f64_values():
     import torch
     from noa_b200 import fourier_project as fp
