@@ -122,6 +122,23 @@ NB_API int nb_insert_central_slices_3d_scatter(
     const nb_transform* fwd_scaling, const nb_transform* inv_rotation,
     const nb_options* options, void* stream);
 
+/* fourier_interpolation_correction (FourierProject.hpp:2062-2087): real-space correction of the LINEAR
+ * gridding kernel, output = input / sinc^2(pi r) (post_correction != 0) or input * sinc^2(pi r), r the
+ * distance of each voxel from the center (shape / 2) in units of the shape. Real f32 arrays; the input
+ * may broadcast (size-1 dimensions) or be a constant, and may be the output (in place). interp must be
+ * NB_INTERP_LINEAR (or its _FAST alias), else NB_ERROR_INVALID, as in the reference. */
+NB_API int nb_fourier_interpolation_correction(const nb_array* input, const nb_array* output, int32_t interp,
+                                               int32_t post_correction, void* stream);
+
+/* Reconstruction spectrum pass (no counterpart in the reference): output = values / max(weights,
+ * weight_threshold) (no division when weights is NULL), remapped from the inserted layout (centered = 1:
+ * "hc", 0: "h") to the non-centered layout a c2r FFT reads, times exp(-2 pi i k.c / n) with c = n / 2,
+ * so that the c2r's real-space origin lands at the volume's center (where nb_fourier_interpolation_correction
+ * puts it). One volume, `volume_shape` {1, D, H, W}; output contiguous c32 and not overlapping the inputs. */
+NB_API int nb_reconstruction_spectrum(const nb_array* values, const nb_array* weights, const int64_t volume_shape[4],
+                                      int32_t centered, double weight_threshold, const nb_array* output,
+                                      void* stream);
+
 /* extract_central_slices_3d: 3-D spectrum interpolation at every pixel of every output slice (=). */
 NB_API int nb_extract_central_slices_3d(
     int32_t remap,

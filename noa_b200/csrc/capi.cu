@@ -476,6 +476,83 @@ using namespace nb;
 
 extern "C" {
 
+int nb_fourier_interpolation_correction(const nb_array* input, const nb_array* output, int32_t interp,
+                                        int32_t post_correction, void* stream) {
+    if (interp_family(interp) != 1)
+        return fail(NB_ERROR_INVALID, "interp=%d is currently not supported (LINEAR only)", interp);
+    if (!is_array(output))
+        return fail(NB_ERROR_INVALID, "output should be an array");
+    if (!present(input))
+        return fail(NB_ERROR_INVALID, "input should not be empty");
+    if (input->dtype != NB_DTYPE_F32 || output->dtype != NB_DTYPE_F32) {
+        if (is_f64(input->dtype) || is_f64(output->dtype))
+            return fail(NB_ERROR_UNSUPPORTED, "f64 values are not provided on the GPU by this library");
+        return fail(NB_ERROR_INVALID, "input and output should be real (f32)");
+    }
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(NB_ERROR_CUDA, "no CUDA device");
+    }
+    for (int i = 0; i < 4; ++i) {
+        if (output->shape[i] <= 0)
+            return fail(NB_ERROR_INVALID, "Empty array detected (output)");
+        if (output->strides[i] < 0 || (!input->is_value && input->strides[i] < 0))
+            return fail(NB_ERROR_INVALID, "negative strides are not supported");
+        if (!input->is_value && input->shape[i] != output->shape[i] && input->shape[i] != 1)
+            return fail(NB_ERROR_INVALID,
+                        "input of shape {%lld,%lld,%lld,%lld} cannot be broadcast to the output shape "
+                        "{%lld,%lld,%lld,%lld}",
+                        (long long) input->shape[0], (long long) input->shape[1], (long long) input->shape[2],
+                        (long long) input->shape[3], (long long) output->shape[0], (long long) output->shape[1],
+                        (long long) output->shape[2], (long long) output->shape[3]);
+    }
+    if (reinterpret_cast<uintptr_t>(output->data) % 4 || (!input->is_value && reinterpret_cast<uintptr_t>(input->data) % 4))
+        return fail(NB_ERROR_INVALID, "misaligned data pointer");
+    int st = check_device_pointer(output->data, "output", device);
+    if (st == NB_OK && !input->is_value)
+        st = check_device_pointer(input->data, "input", device);
+    if (st != NB_OK)
+        return st;
+    return finish(launch_gridding_correction(input, output, post_correction != 0, static_cast<cudaStream_t>(stream)));
+}
+
+int nb_reconstruction_spectrum(const nb_array* values, const nb_array* weights, const int64_t volume_shape[4],
+                               int32_t centered, double weight_threshold, const nb_array* output, void* stream) {
+    if (!volume_shape)
+        return fail(NB_ERROR_INVALID, "volume_shape should not be NULL");
+    if (volume_shape[0] != 1)
+        return fail(NB_ERROR_INVALID, "one volume at a time, got a batch of %lld", (long long) volume_shape[0]);
+    if (!is_array(values) || values->dtype != NB_DTYPE_C32)
+        return fail(NB_ERROR_INVALID, "values should be a complex (c32) array");
+    if (!is_array(output) || output->dtype != NB_DTYPE_C32)
+        return fail(NB_ERROR_INVALID, "output should be a complex (c32) array");
+    if (present(weights) && (!is_array(weights) || weights->dtype != NB_DTYPE_F32))
+        return fail(NB_ERROR_INVALID, "weights should be a real (f32) array or absent");
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(NB_ERROR_CUDA, "no CUDA device");
+    }
+    int st = check_array(values, volume_shape, "values", false, device);
+    if (st == NB_OK)
+        st = check_array(weights, volume_shape, "weights", true, device);
+    if (st == NB_OK)
+        st = check_array(output, volume_shape, "output", false, device);
+    if (st != NB_OK)
+        return st;
+    const int64_t wp = volume_shape[3] / 2 + 1;
+    if (output->strides[3] != 1 || output->strides[2] != wp || output->strides[1] != wp * volume_shape[2])
+        return fail(NB_ERROR_INVALID, "output should be contiguous");
+    if (overlap(output, values) || overlap(output, weights))
+        return fail(NB_ERROR_INVALID, "output should not overlap the inputs");
+    if (static_cast<int64_t>(volume_shape[1]) * volume_shape[2] * wp >= (int64_t(1) << 31))
+        return fail(NB_ERROR_INVALID, "the volume must span fewer than 2^31 elements");
+    return finish(launch_reconstruction_spectrum(values, present(weights) ? weights : nullptr, volume_shape,
+                                                 centered != 0, static_cast<float>(weight_threshold), output,
+                                                 static_cast<cudaStream_t>(stream)));
+}
+
 int64_t nb_volume_pairs_bytes(const int64_t volume_shape[4]) {
     if (!volume_shape || volume_shape[1] <= 0 || volume_shape[2] <= 0 || volume_shape[3] <= 0)
         return -1;

@@ -44,6 +44,13 @@ cudaError_t launch_rasterize(const ProjArgs& a, cudaStream_t stream);
 cudaError_t launch_insert(const ProjArgs& a, cudaStream_t stream);
 cudaError_t launch_insert_extract(const ProjArgs& a, cudaStream_t stream);
 cudaError_t launch_insert_scatter(const ProjArgs& a, cudaStream_t stream);
+// The reconstruction's spectrum pass (fp_reconstruct.cu) on checked arrays.
+cudaError_t launch_reconstruction_spectrum(const nb_array* values, const nb_array* weights,
+                                           const int64_t shape[4], bool centered, float threshold,
+                                           const nb_array* out, cudaStream_t stream);
+// fourier_interpolation_correction on checked real f32 arrays (capi.cu checks them).
+cudaError_t launch_gridding_correction(const nb_array* input, const nb_array* output, bool post,
+                                       cudaStream_t stream);
 
 // Argument checks and per-call constants of nb_rasterize_central_slices_3d (capi.cu); fills `a` and
 // returns NB_OK, or an NB_ERROR_* code with the thread's last-error message set.

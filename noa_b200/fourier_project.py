@@ -82,6 +82,8 @@ def lib() -> C.CDLL:
                   "nb_insert_central_slices_3d", "nb_insert_central_slices_3d_scatter",
                   "nb_extract_central_slices_3d", "nb_insert_and_extract_central_slices_3d"):
             getattr(h, f).restype = C.c_int
+        h.nb_fourier_interpolation_correction.argtypes = [arr, arr, C.c_int32, C.c_int32, C.c_void_p]
+        h.nb_fourier_interpolation_correction.restype = C.c_int
         h.nb_last_error.restype = C.c_char_p
         h.nb_version.restype = C.c_char_p
         h.nb_options_default.argtypes = [opt]
@@ -296,6 +298,17 @@ def insert_central_slices_3d_scatter(remap: str, slice, slice_weight, slice_shap
         _ref(as_nb_array(volume, keep)), _ref(as_nb_array(volume_weight, keep)), _shape(volume_shape),
         _ref(as_nb_transform(fwd_scaling, False, keep)), _ref(as_nb_transform(inv_rotation, True, keep)),
         C.byref(o), _stream_ptr(stream)))
+
+
+def fourier_interpolation_correction(input, output, interp="linear", post_correction=True, *, stream=None) -> None:
+    """noa::xform::fourier_interpolation_correction (FourierProject.hpp:2062-2087): divides (post) or
+    multiplies (pre) the real-space ``input`` by sinc^2(pi r) into ``output`` (4-D float32 CUDA tensors,
+    ``input`` broadcastable or a float; in place allowed). LINEAR only, as in the reference."""
+    keep = []
+    _check(lib().nb_fourier_interpolation_correction(
+        _ref(as_nb_array(input, keep)), _ref(as_nb_array(output, keep)),
+        INTERPS[interp] if isinstance(interp, str) else int(interp), int(bool(post_correction)),
+        _stream_ptr(stream)))
 
 
 def extract_central_slices_3d(remap: str, volume, volume_weight, volume_shape, slice, slice_weight, slice_shape,

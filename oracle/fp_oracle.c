@@ -14,6 +14,7 @@
 #define R_SIN sinf
 #define R_COS cosf
 #define R_FABS fabsf
+#define R_SQRT sqrtf
 #define R_EPS FLT_EPSILON
 #define R_MAT33_STRIDE 12
 #include "fp_oracle_impl.h"
@@ -24,6 +25,7 @@
 #undef R_SIN
 #undef R_COS
 #undef R_FABS
+#undef R_SQRT
 #undef R_EPS
 #undef R_MAT33_STRIDE
 
@@ -34,6 +36,7 @@
 #define R_SIN sin
 #define R_COS cos
 #define R_FABS fabs
+#define R_SQRT sqrt
 #define R_EPS DBL_EPSILON
 #define R_MAT33_STRIDE 10
 #include "fp_oracle_impl.h"

@@ -76,6 +76,17 @@ FPO_DECLARE(fpo_extract, _f64);
 FPO_DECLARE(fpo_insert_extract, _f32);
 FPO_DECLARE(fpo_insert_extract, _f64);
 
+/* fourier_interpolation_correction (FourierProject.hpp:2062-2087; GriddingCorrection :1009-1061):
+ * real input and output arrays (`input` may broadcast with zero strides) of the output's BDHW shape;
+ * interp must be LINEAR (1 or 101). post_correction != 0 divides by sinc^2(pi r), else multiplies.
+ * PARITY UNPINNED: the reference's GriddingCorrection does not compile (FourierProject.hpp:1034 builds
+ * `half` with Vec::from_vec(l_shape != 1), but Shape's != yields one bool), no test or caller of it
+ * exists, so this restates its documented intent: half = shape / 2 (float), 0 where a size is 1. */
+int fpo_gridding_correction_f32(const fpo_array* input, const fpo_array* output, int32_t interp,
+                                int32_t post_correction, int n_threads);
+int fpo_gridding_correction_f64(const fpo_array* input, const fpo_array* output, int32_t interp,
+                                int32_t post_correction, int n_threads);
+
 #ifdef __cplusplus
 }
 #endif

@@ -800,6 +800,47 @@ FPO_DECLARE_X(fpo_insert_extract, SFX) {
     return 0;
 }
 
+/* ------------------------------------------------------------------------------------------------
+ * fourier_interpolation_correction (FourierProject.hpp:2062-2087) with GriddingCorrection
+ * (:1009-1061): per voxel, dist = ((j, k, l) - half) / shape with half = shape / 2 (0 where a size is
+ * 1), r = |dist|, sinc2 = sinc(pi r)^2 (noa::sinc: 1 at 0, base/Math.hpp:28-29); the output is
+ * value / sinc2 (post-correction) or value * sinc2.
+ * ------------------------------------------------------------------------------------------------ */
+int F_(fpo_gridding_correction)(const fpo_array* input, const fpo_array* output, int32_t interp,
+                                int32_t post_correction, int n_threads) {
+    if (!input || !output || !output->data || (!input->data && !input->is_value))
+        return -1;
+    if (interp != 1 && interp != 101)
+        return -2;
+    const int64_t* sh = output->shape;
+    const R fs[3] = {(R) sh[1], (R) sh[2], (R) sh[3]};
+    R half[3];
+    for (int i = 0; i < 3; ++i)
+        half[i] = fs[i] / (R) 2 * (R) (sh[i + 1] != 1);
+    const R PI = (R) 3.14159265358979323846;
+    R* out = (R*) output->data;
+    const R* in = (const R*) input->data;
+    (void) n_threads;
+    for (int64_t b = 0; b < sh[0]; ++b)
+        for (int64_t j = 0; j < sh[1]; ++j)
+            for (int64_t k = 0; k < sh[2]; ++k)
+                for (int64_t l = 0; l < sh[3]; ++l) {
+                    R d0 = (R) j, d1 = (R) k, d2 = (R) l;
+                    d0 -= half[0]; d1 -= half[1]; d2 -= half[2];
+                    d0 /= fs[0]; d1 /= fs[1]; d2 /= fs[2];
+                    const R radius = R_SQRT(d0 * d0 + d1 * d1 + d2 * d2);
+                    const R x = PI * radius;
+                    const R sinc = x == 0 ? (R) 1 : R_SIN(x) / x;
+                    const R sinc2 = sinc * sinc;
+                    const R v = input->is_value ? (R) input->value[0]
+                                                : in[b * input->strides[0] + j * input->strides[1] +
+                                                     k * input->strides[2] + l * input->strides[3]];
+                    out[b * output->strides[0] + j * output->strides[1] + k * output->strides[2] +
+                        l * output->strides[3]] = post_correction ? v / sinc2 : v * sinc2;
+                }
+    return 0;
+}
+
 #undef cpx_t
 #undef FPO_DECLARE_X
 #undef F_

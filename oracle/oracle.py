@@ -195,6 +195,21 @@ class FpOracle(_Lib):
         return fn(*args)
 
 
+def gridding_correction(inp, out: np.ndarray, interp: int = 1, post_correction: bool = True,
+                        threads: int = 1) -> int:
+    """fpo_gridding_correction_{f32,f64} on host arrays (``inp`` an array or a float constant)."""
+    lib = FpOracle().lib
+    keep = []
+    f64 = out.dtype == np.float64
+    fn = getattr(lib, f"fpo_gridding_correction_{'f64' if f64 else 'f32'}")
+    if isinstance(inp, (int, float)):
+        a = _fpo_array(None, keep, value=float(inp), value_shape=out.shape, complex_value=False)
+    else:
+        a = _fpo_array(inp, keep)
+    o = _fpo_array(out, keep)
+    return fn(C.byref(a), C.byref(o), C.c_int32(interp), C.c_int32(int(post_correction)), C.c_int(threads))
+
+
 COMBOS = {("c32", "c32"): 0, ("f32", "f32"): 1, ("c32", "f32"): 2, ("c64", "c64"): 3, ("f64", "f64"): 4}
 _DT = {np.dtype(np.complex64): "c32", np.dtype(np.float32): "f32",
        np.dtype(np.complex128): "c64", np.dtype(np.float64): "f64"}

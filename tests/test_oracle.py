@@ -102,3 +102,37 @@ def test_known_answer_identity_extract():
     f = synthetic.slice_fftfreq_norm((n, n), centered=True)
     expected = np.where(f <= 0.5, vol[0, n // 2], 0)
     np.testing.assert_allclose(call.out[0, 0], expected, rtol=0, atol=0)
+
+
+# ---------------------------------------------------------------------------------------------------
+# Gridding correction. The reference's GriddingCorrection does not compile (FourierProject.hpp:1034),
+# so the oracle is checked against an independent numpy restatement of its documented formula.
+# ---------------------------------------------------------------------------------------------------
+def _numpy_gridding(inp, shape, post):
+    b, d, h, w = shape
+    half = np.array([s / 2 if s != 1 else 0.0 for s in (d, h, w)])
+    j, k, l = np.meshgrid(np.arange(d), np.arange(h), np.arange(w), indexing="ij")
+    dist = np.stack([(j - half[0]) / d, (k - half[1]) / h, (l - half[2]) / w])
+    x = np.pi * np.sqrt((dist ** 2).sum(0))
+    with np.errstate(invalid="ignore", divide="ignore"):
+        sinc = np.where(x == 0, 1.0, np.sin(x) / x)
+    s2 = np.broadcast_to(sinc ** 2, shape)
+    v = np.broadcast_to(np.asarray(inp, dtype=np.float64), shape)
+    return v / s2 if post else v * s2
+
+
+@pytest.mark.parametrize("shape", [(1, 16, 16, 16), (2, 9, 12, 7), (1, 1, 20, 20), (1, 24, 1, 1)])
+@pytest.mark.parametrize("post", [True, False])
+def test_oracle_gridding_matches_formula(shape, post):
+    from oracle.oracle import gridding_correction
+    rng = np.random.default_rng(sum(shape))
+    inp = rng.standard_normal(shape)
+    for dt, tol in ((np.float32, 2e-6), (np.float64, 1e-12)):
+        out = np.zeros(shape, dtype=dt)
+        assert gridding_correction(inp.astype(dt), out, post_correction=post) == 0
+        ref = _numpy_gridding(inp.astype(dt).astype(np.float64), shape, post)
+        assert np.max(np.abs(out - ref) / np.maximum(np.abs(ref), 1e-30)) < tol
+    out = np.zeros(shape, dtype=np.float32)
+    assert gridding_correction(2.5, out, post_correction=post) == 0
+    assert np.allclose(out, _numpy_gridding(2.5, shape, post), rtol=2e-6)
+    assert gridding_correction(inp.astype(np.float32), out, interp=2) == -2  # LINEAR only
