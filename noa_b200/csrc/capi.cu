@@ -444,6 +444,8 @@ int prepare_insert(
     if (t[2] < tmin) tmin = t[2];
     a.fs = fmax_ref(static_cast<float>(options->fftfreq_sinc), 1.f / tmin);
     a.fb = fmax_ref(static_cast<float>(options->fftfreq_blackman), 1.f / tmin);
+    a.pfs = static_cast<float>(3.14159265358979323846 / static_cast<double>(a.fs));
+    a.pfb = static_cast<float>(3.14159265358979323846 / static_cast<double>(a.fb));
     a.in_cplx = is_complex(slice->dtype);
     a.out_cplx = is_complex(volume->dtype);
     return NB_OK;
@@ -711,6 +713,8 @@ int nb_insert_and_extract_central_slices_3d(
     a.vz = vz;
     a.fs = fmax_ref(static_cast<float>(options->fftfreq_sinc), 1.f / vz);
     a.fb = fmax_ref(static_cast<float>(options->fftfreq_blackman), 1.f / vz);
+    a.pfs = static_cast<float>(3.14159265358979323846 / static_cast<double>(a.fs));
+    a.pfb = static_cast<float>(3.14159265358979323846 / static_cast<double>(a.fb));
     a.efs = fmax_ref(static_cast<float>(options->w_fftfreq_sinc), 1.f / vz);
     a.efb = fmax_ref(static_cast<float>(options->w_fftfreq_blackman), 1.f / vz);
     a.wsize = blackman_window_size(a.efb, vz);

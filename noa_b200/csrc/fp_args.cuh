@@ -30,6 +30,7 @@ struct ProjArgs {
     float target0, target1, target2;
     float cutoff_sqd;
     float fs, fb;              // windowed sinc (insert; insert_extract input)
+    float pfs, pfb;            // pi / fs, pi / fb (for windowed_sinc_fast)
     float efs, efb;            // w-windowed sinc (extract; insert_extract output)
     int wsize;                 // w-window size (1 = plain 3-D form)
     float vz;                  // insert_extract: the virtual volume's z size
