@@ -16,6 +16,7 @@
 #pragma once
 
 #include <noa/xform/FourierProject.hpp>
+#include <noa/xform/Texture.hpp>
 
 #include "noa_b200/fourier_project.h"
 
@@ -101,6 +102,50 @@ namespace noa_b200::binding {
         return t;
     }
 
+    // An input that may be a Texture (Texture.hpp). noa keeps a GPU texture's values in a CUDA array
+    // (Texture.hpp:147-170); the binding copies them into linear device memory with one
+    // cudaMemcpy3DAsync on the call's stream (a 3-D array for a volume, a layered 2-D array for a stack
+    // of slices: extent W x H x (B*D) either way), keeps that buffer alive on the stream, and passes it
+    // as an array. Views, values and Empty pass through unchanged.
+    template<typename T>
+    struct Staged {
+        using d = std::decay_t<T>;
+        static constexpr bool TEXTURE = nt::texture<d>;
+        nb_array array{};
+        std::conditional_t<TEXTURE, ::noa::Array<nt::mutable_value_type_t<d>>, int> keep{};
+    };
+
+    template<typename T>
+    Staged<T> stage(const T& a, void* stream) {
+        Staged<T> s;
+        if constexpr (Staged<T>::TEXTURE) {
+#ifdef NOA_ENABLE_CUDA
+            using V = nt::mutable_value_type_t<std::decay_t<T>>;
+            const ::noa::Shape4 shape = a.shape();
+            s.keep = ::noa::Array<V>(shape, ::noa::ArrayOption{a.device(), ::noa::Allocator::DEFAULT});
+            cudaMemcpy3DParms p{};
+            p.srcArray = a.cuda().handle->array.get();
+            p.dstPtr = make_cudaPitchedPtr(s.keep.get(), static_cast<size_t>(shape[3]) * sizeof(V),
+                                           static_cast<size_t>(shape[3]), static_cast<size_t>(shape[2]));
+            p.extent = make_cudaExtent(static_cast<size_t>(shape[3]), static_cast<size_t>(shape[2]),
+                                       static_cast<size_t>(shape[0] * shape[1]));
+            p.kind = cudaMemcpyDeviceToDevice;
+            const cudaError_t err = cudaMemcpy3DAsync(&p, static_cast<cudaStream_t>(stream));
+            if (err != cudaSuccess)
+                ::noa::panic("noa_b200: staging a texture failed: {}", cudaGetErrorString(err));
+            ::noa::Stream::current(a.device()).cuda().enqueue_attach(s.keep);
+            s.array = to_array(s.keep.view());
+#else
+            (void) stream;
+            ::noa::panic("noa_b200: texture inputs need noa's CUDA backend");
+#endif
+        } else {
+            (void) stream;
+            s.array = to_array(a);
+        }
+        return s;
+    }
+
     inline void fill_common(nb_options& o, double cutoff, const ::noa::Shape4& target, const ::noa::Vec<double, 2>& ews) {
         nb_options_default(&o);
         o.fftfreq_cutoff = cutoff;
@@ -142,13 +187,18 @@ namespace noa_b200::binding {
                 const nx::InsertCentralSlicesOptions& options, void* stream) {
         nb_options o;
         fill_common(o, options.fftfreq_cutoff, options.target_shape, options.ews_radius);
-        o.interp = static_cast<int32_t>(options.interp.value);
+        // With textures, the interpolation method is the textures' (FourierProject.hpp:1203-1217).
+        o.interp = static_cast<int32_t>(
+            nx::details::fourier_insert_extract_interp_mode(slice, slice_weight, options.interp).value);
         o.fftfreq_sinc = options.windowed_sinc.fftfreq_sinc;
         o.fftfreq_blackman = options.windowed_sinc.fftfreq_blackman;
-        const nb_array s = to_array(slice), sw = to_array(slice_weight), v = to_array(volume), vw = to_array(volume_weight);
+        const auto s = stage(slice, stream);
+        const auto sw = stage(slice_weight, stream);
+        const nb_array v = to_array(volume), vw = to_array(volume_weight);
         const nb_transform sc = to_transform(fwd_scaling), rot = to_transform(inv_rotation);
-        check(nb_insert_central_slices_3d(static_cast<int32_t>(REMAP.value), &s, &sw, shape_ptr(slice_shape),
-                                          &v, &vw, shape_ptr(volume_shape), &sc, &rot, &o, stream));
+        check(nb_insert_central_slices_3d(static_cast<int32_t>(REMAP.value), &s.array, &sw.array,
+                                          shape_ptr(slice_shape), &v, &vw, shape_ptr(volume_shape), &sc, &rot, &o,
+                                          stream));
     }
 
     template<nf::Layout REMAP, typename Input, typename InputWeight, typename Output, typename OutputWeight,
@@ -159,13 +209,17 @@ namespace noa_b200::binding {
                  const nx::ExtractCentralSlicesOptions& options, void* stream) {
         nb_options o;
         fill_common(o, options.fftfreq_cutoff, options.target_shape, options.ews_radius);
-        o.interp = static_cast<int32_t>(options.interp.value);
+        o.interp = static_cast<int32_t>(
+            nx::details::fourier_insert_extract_interp_mode(volume, volume_weight, options.interp).value);
         o.w_fftfreq_sinc = options.w_windowed_sinc.fftfreq_sinc;
         o.w_fftfreq_blackman = options.w_windowed_sinc.fftfreq_blackman;
-        const nb_array v = to_array(volume), vw = to_array(volume_weight), s = to_array(slice), sw = to_array(slice_weight);
+        const auto v = stage(volume, stream);
+        const auto vw = stage(volume_weight, stream);
+        const nb_array s = to_array(slice), sw = to_array(slice_weight);
         const nb_transform sc = to_transform(inv_scaling), rot = to_transform(fwd_rotation);
-        check(nb_extract_central_slices_3d(static_cast<int32_t>(REMAP.value), &v, &vw, shape_ptr(volume_shape),
-                                           &s, &sw, shape_ptr(slice_shape), &sc, &rot, &o, stream));
+        check(nb_extract_central_slices_3d(static_cast<int32_t>(REMAP.value), &v.array, &vw.array,
+                                           shape_ptr(volume_shape), &s, &sw, shape_ptr(slice_shape), &sc, &rot, &o,
+                                           stream));
     }
 
     template<nf::Layout REMAP, typename Input, typename InputWeight, typename Output, typename OutputWeight,
@@ -177,18 +231,21 @@ namespace noa_b200::binding {
                             const nx::InsertAndExtractCentralSlicesOptions& options, void* stream) {
         nb_options o;
         fill_common(o, options.fftfreq_cutoff, ::noa::Shape4{}, options.ews_radius);
-        o.interp = static_cast<int32_t>(options.interp.value);
+        o.interp = static_cast<int32_t>(
+            nx::details::fourier_insert_extract_interp_mode(input_slice, input_weight, options.interp).value);
         o.fftfreq_sinc = options.input_windowed_sinc.fftfreq_sinc;
         o.fftfreq_blackman = options.input_windowed_sinc.fftfreq_blackman;
         o.w_fftfreq_sinc = options.w_windowed_sinc.fftfreq_sinc;
         o.w_fftfreq_blackman = options.w_windowed_sinc.fftfreq_blackman;
         o.add_to_output = options.add_to_output;
         o.correct_weights = options.correct_weights;
-        const nb_array i = to_array(input_slice), iw = to_array(input_weight);
+        const auto i = stage(input_slice, stream);
+        const auto iw = stage(input_weight, stream);
         const nb_array out = to_array(output_slice), ow = to_array(output_weight);
         const nb_transform isc = to_transform(input_fwd_scaling), irot = to_transform(input_inv_rotation);
         const nb_transform osc = to_transform(output_inv_scaling), orot = to_transform(output_fwd_rotation);
-        check(nb_insert_and_extract_central_slices_3d(static_cast<int32_t>(REMAP.value), &i, &iw, shape_ptr(input_shape),
+        check(nb_insert_and_extract_central_slices_3d(static_cast<int32_t>(REMAP.value), &i.array, &iw.array,
+                                                      shape_ptr(input_shape),
                                                       &out, &ow, shape_ptr(output_shape), &isc, &irot, &osc, &orot,
                                                       &o, stream));
     }

@@ -26,3 +26,16 @@ void instantiate(View<const c32> vol, View<const f32> volw, View<c32> slices, Vi
     bind::insert_and_extract<"hc2h">(in_slices, Empty{}, sshape, slices, slices_w, sshape, Empty{}, rot, scale, quat,
                                      nx::InsertAndExtractCentralSlicesOptions{.correct_weights = true}, stream);
 }
+
+// Texture inputs (staged into linear memory by the binding; with NOA_ENABLE_CUDA through the CUDA array).
+void instantiate_textures(const nx::Texture<c32>& tvol, const nx::Texture<f32>& tvolw, const nx::Texture<c32>& tslices,
+                          View<c32> slices, View<f32> slices_w, View<const Mat33<f32>> rot, View<c32> grid,
+                          View<f32> grid_w, void* stream) {
+    const Shape4 vshape{1, 8, 8, 8}, sshape{2, 1, 8, 8};
+    bind::extract<"hc2h">(tvol, tvolw, vshape, slices, slices_w, sshape, Empty{}, rot,
+                          nx::ExtractCentralSlicesOptions{}, stream);
+    bind::insert<"hc2hc">(tslices, Empty{}, sshape, grid, grid_w, vshape, Empty{}, rot,
+                          nx::InsertCentralSlicesOptions{}, stream);
+    bind::insert_and_extract<"hc2h">(tslices, Empty{}, sshape, slices, slices_w, sshape, Empty{}, rot, Empty{}, rot,
+                                     nx::InsertAndExtractCentralSlicesOptions{}, stream);
+}
