@@ -276,6 +276,22 @@ class ProjectionServer:
         self.resident += vol.nbytes
         return vol
 
+    def add_volume_file(self, vid: int, path: str, logical_width: int | None = None) -> Volume:
+        """Makes an rfft volume stored in an MRC file (mode 4, complex64, physical shape
+        (1, D, H, W/2+1)) resident on the executor's device. The logical width defaults to the even
+        W = 2 (W/2+1 - 1)."""
+        import torch
+        from . import mrc
+        data, h = mrc.read(path)
+        if data.dtype != np.complex64 or data.shape[0] != 1:
+            raise ValueError(f"{path}: expected one complex64 rfft volume, got {data.dtype} {data.shape}")
+        _, d, hh, wp = data.shape
+        w = logical_width if logical_width is not None else 2 * (wp - 1)
+        if w // 2 + 1 != wp:
+            raise ValueError(f"{path}: width {wp} is not the rfft width of {w}")
+        device = getattr(self.ex, "device", "cuda")
+        return self.add_volume(vid, torch.from_numpy(np.ascontiguousarray(data)).to(device), (1, d, hh, w))
+
     # -- requests ------------------------------------------------------------------------------------
     def submit(self, req: Request) -> Request:
         if req.kind not in ("extract", "insert"):

@@ -208,3 +208,19 @@ def test_run_stream_real_time_with_instant_executor():
     assert all(r.error is None and r.done >= r.arrival for r in reqs)
     assert s.stats.completed == 20
     assert t1 >= t0
+
+
+def test_add_volume_file_reads_an_mrc_rfft_volume(tmp_path):
+    import torch
+    from noa_b200 import mrc
+    vol = (np.arange(8 * 8 * 5, dtype=np.float32).reshape(1, 8, 8, 5) * (1 + 1j)).astype(np.complex64)
+    p = str(tmp_path / "v.mrc")
+    mrc.write(p, vol)
+    clock = Clock()
+    ex = FakeExecutor(clock)
+    ex.device = "cpu"
+    s = ProjectionServer(ex, 10 ** 9, clock=clock)
+    v = s.add_volume_file(3, p)
+    assert v.shape == (1, 8, 8, 8) and torch.equal(v.data, torch.from_numpy(vol))
+    with pytest.raises(ValueError):
+        s.add_volume_file(4, p, logical_width=10)
