@@ -505,7 +505,7 @@ def main() -> None:
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--ref-batch", type=int, default=32)
-    p.add_argument("--n", type=int, default=256, help="box size (profiling runs use smaller cases)")
+    p.add_argument("--n", type=int, default=None, help="box size (default 256, or 512 for insert_512)")
     p.add_argument("--slices", type=int, default=None, help="slices per op per step")
     p.add_argument("--workload", choices=["extract_insert_256", "insert_512"], default="extract_insert_256",
                    help="insert_512: the 512^3 x 20,000 windowed-sinc insertion, gather vs scatter form")
@@ -513,12 +513,12 @@ def main() -> None:
     args = p.parse_args()
     global N, SLICES
     if args.workload == "insert_512":
-        args.n = 512 if args.n == 256 else args.n
+        args.n = args.n or 512
         args.slices = args.slices or 20000
         args.steps = min(args.steps, 3)
         run_large(args)
         return
-    N, SLICES = args.n, args.slices or 4096
+    N, SLICES = args.n or 256, args.slices or 4096
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
