@@ -207,6 +207,14 @@ Ews make_ews(const double r[2]) {
 
 float fmax_ref(float a, float b) { return a < b ? b : a; }
 
+// Whether offsets within one slice (dimensions 2 and 3) of an array fit 31 bits.
+bool slice_narrow(const nb_array* a) {
+    if (!is_array(a))
+        return false;
+    const int64_t extent = (a->shape[2] - 1) * a->strides[2] + (a->shape[3] - 1) * a->strides[3];
+    return extent < (int64_t(1) << 31) - 1 && a->strides[2] < (int64_t(1) << 31) && a->strides[3] < (int64_t(1) << 31);
+}
+
 // Whether an array's largest element offset needs more than 31 bits.
 bool needs_wide(const nb_array* a) {
     if (!is_array(a))
@@ -446,6 +454,7 @@ int prepare_insert(
     a.fb = fmax_ref(static_cast<float>(options->fftfreq_blackman), 1.f / tmin);
     a.pfs = static_cast<float>(3.14159265358979323846 / static_cast<double>(a.fs));
     a.pfb = static_cast<float>(3.14159265358979323846 / static_cast<double>(a.fb));
+    a.in_slice_narrow = slice_narrow(slice) && (!is_array(slice_weight) || slice_narrow(slice_weight));
     a.in_cplx = is_complex(slice->dtype);
     a.out_cplx = is_complex(volume->dtype);
     return NB_OK;
@@ -720,6 +729,7 @@ int nb_insert_and_extract_central_slices_3d(
     a.wsize = blackman_window_size(a.efb, vz);
     a.add_to_output = options->add_to_output != 0;
     a.correct_weights = options->correct_weights != 0;
+    a.in_slice_narrow = slice_narrow(input_slice) && (!is_array(input_weight) || slice_narrow(input_weight));
     a.in_cplx = is_complex(input_slice->dtype);
     a.out_cplx = is_complex(output_slice->dtype);
     return finish(launch_insert_extract(a, static_cast<cudaStream_t>(stream)));

@@ -38,6 +38,7 @@ struct ProjArgs {
 
     int in_cplx, out_cplx;     // value kinds (input/output complex?)
     int wide_in;               // input offsets need 64 bits (an array spans >= 2^31 elements)
+    int in_slice_narrow;       // offsets within one input slice fit 32 bits
 };
 
 cudaError_t launch_extract(const ProjArgs& a, cudaStream_t stream);

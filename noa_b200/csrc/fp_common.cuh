@@ -285,7 +285,37 @@ __device__ __forceinline__ float2 cfma(float2 a, float s, float2 acc) {
 
 // Spectrum geometry of one rfft input: logical sizes (last one is the full width) and centering.
 struct Spectrum3 { int n0, n1, n2; bool centered; };
-struct Spectrum2 { int n0, n1; bool centered; };
+struct Spectrum2 { int n0, n1; bool centered; bool narrow = false; };  // narrow: in-slice offsets fit 32 bits
+
+// Reads elements of one slice of a stack: with `narrow`, from the slice's base pointer with 32-bit
+// in-slice offsets (the stack itself may span more than 2^31 elements); else through src_read.
+template<bool CPLX>
+struct SliceReader {
+    const SrcView& src;
+    int64_t batch;
+    const void* base;
+    int s1, s2;
+    bool narrow;
+
+    __device__ __forceinline__ SliceReader(const SrcView& s, int64_t b, bool n)
+        : src(s), batch(b), narrow(n && !s.is_value) {
+        base = narrow ? static_cast<const void*>(static_cast<const char*>(s.data) +
+                                                 b * s.s0 * static_cast<int64_t>(CPLX ? sizeof(float2) : sizeof(float)))
+                      : nullptr;
+        s1 = static_cast<int>(s.s1);
+        s2 = static_cast<int>(s.s2);
+    }
+    __device__ __forceinline__ float2 operator()(int i1, int i2) const {
+        if (narrow) {
+            const int off = i1 * s1 + i2 * s2;
+            if constexpr (CPLX)
+                return __ldg(static_cast<const float2*>(base) + off);
+            else
+                return make_float2(__ldg(static_cast<const float*>(base) + off), 0.f);
+        }
+        return src_read<CPLX>(src, batch, i1, i2);
+    }
+};
 
 // ---------------------------------------------------------------------------------------------------
 // interpolate_spectrum, 3-D (volume) form. `freq` is in samples, centered on DC.
@@ -364,6 +394,7 @@ __device__ __forceinline__ float2 interp_spectrum_2d(const SrcView& src, const S
     constexpr bool FLIP_EARLY = SIZE <= 2;
     const int lo0 = -sp.n0 / 2, hi0 = (sp.n0 - 1) / 2;
     const int hi1 = sp.n1 / 2;
+    const SliceReader<CPLX> read(src, batch, sp.narrow);
     float conjugate = 1.f;
     if (FLIP_EARLY && f1 < 0.f) {
         f0 = -f0; f1 = -f1;
@@ -374,7 +405,7 @@ __device__ __forceinline__ float2 interp_spectrum_2d(const SrcView& src, const S
         const int i1 = static_cast<int>(roundf(f1));
         float2 v = make_float2(0.f, 0.f);
         if (i0 >= lo0 && i0 <= hi0 && i1 >= 0 && i1 <= hi1)
-            v = src_read<CPLX>(src, batch, frequency2index(sp.centered, i0, sp.n0), i1);
+            v = read(frequency2index(sp.centered, i0, sp.n0), i1);
         return v;
     } else {
         constexpr int START = -(SIZE - 1) / 2;
@@ -394,7 +425,7 @@ __device__ __forceinline__ float2 interp_spectrum_2d(const SrcView& src, const S
                     float2 vy = make_float2(0.f, 0.f);
 #pragma unroll
                     for (int x = 0; x < SIZE; ++x)
-                        vy = cfma(src_read<CPLX>(src, batch, iy, b1 + START + x), w1[x], vy);
+                        vy = cfma(read(iy, b1 + START + x), w1[x], vy);
                     value = cfma(vy, w0[y], value);
                 }
                 return value;
@@ -412,7 +443,7 @@ __device__ __forceinline__ float2 interp_spectrum_2d(const SrcView& src, const S
                     conj = -1.f;
                 }
                 if (t0 >= lo0 && t0 <= hi0 && t1 >= 0 && t1 <= hi1) {
-                    float2 v = src_read<CPLX>(src, batch, frequency2index(sp.centered, t0, sp.n0), t1);
+                    float2 v = read(frequency2index(sp.centered, t0, sp.n0), t1);
                     if (!FLIP_EARLY)
                         v.y *= conj;
                     vy = cfma(v, w1[x], vy);

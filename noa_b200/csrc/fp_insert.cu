@@ -26,7 +26,7 @@ insert_kernel(const __grid_constant__ ProjArgs a, int nbz, int nby, int nbx) {
 
     const int D = a.vol_d, H = a.vol_h, WP = a.vol_w / 2 + 1;
     const bool vc = a.out_centered;
-    const Spectrum2 sp{a.slice_h, a.slice_w, a.in_centered};
+    const Spectrum2 sp{a.slice_h, a.slice_w, a.in_centered, a.in_slice_narrow != 0};
     const bool has_out_w = a.out_w.present;
     const bool has_in_w = a.in_w.present;
     const int tid = threadIdx.x;

@@ -39,7 +39,7 @@ insert_extract_kernel(const __grid_constant__ ProjArgs a, int tiles_per_slice, i
 
     const int wp = a.slice_w / 2 + 1;
     const int plane = a.slice_h * wp;
-    const Spectrum2 sp{a.in_h, a.in_w_, a.in_centered};
+    const Spectrum2 sp{a.in_h, a.in_w_, a.in_centered, a.in_slice_narrow != 0};
     const bool has_out_w = a.out_w.present;
     const bool has_in_w = a.in_w.present;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;

@@ -48,7 +48,7 @@ __global__ void __launch_bounds__(SCATTER_THREADS)
 insert_scatter_kernel(const __grid_constant__ ProjArgs a, void* __restrict__ acc) {
     const int D = a.vol_d, H = a.vol_h, WP = a.vol_w / 2 + 1;
     const bool vc = a.out_centered;
-    const Spectrum2 sp{a.slice_h, a.slice_w, a.in_centered};
+    const Spectrum2 sp{a.slice_h, a.slice_w, a.in_centered, a.in_slice_narrow != 0};
     const bool has_in_w = a.in_w.present;
     // Frequency ranges: z in [-D/2, (D-1)/2], y in [-H/2, (H-1)/2], x in [0, W/2].
     auto lo_of = [&](int axis) { return axis == 0 ? -D / 2 : axis == 1 ? -H / 2 : 0; };
