@@ -2,11 +2,13 @@
 // counts — executed by ONE persistent kernel, replayed as a CUDA graph.
 //
 // Work decomposition: every request is cut into (slice, tile) items, a tile being TY x TX pixels of
-// one output slice. Items are numbered request after request; a device counter hands them out, one
-// per CTA at a time (atomicAdd), so uneven requests balance themselves across the SMs without a
-// per-request launch. Each item runs the same per-pixel code as nb_extract_central_slices_3d's
-// generic path (extract_one below restates that kernel body for a single pixel), so results are
-// bit-identical to the per-call entry point.
+// one output slice (4 TY x TX for a request read through its volume's pair copy, 4 rows per thread).
+// Items are numbered request after request; a device counter hands them out, one per CTA at a time
+// (atomicAdd), so uneven requests balance themselves across the SMs without a per-request launch. A
+// CTA stages the descriptor of its current request in shared memory. Each item runs the per-pixel
+// code of nb_extract_central_slices_3d (extract_one restates the generic kernel body for one pixel,
+// extract_rows_pairs the pair-copy kernel body for 4 rows), so results are bit-identical to the
+// per-call entry point.
 //
 // nb_extract_batch_create validates every request like the per-call entry point, uploads the request
 // descriptors once, optionally autotunes (tile shape x CTAs per SM, timed on the batch itself and

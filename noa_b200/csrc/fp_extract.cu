@@ -3,9 +3,11 @@
 //
 // Work decomposition: a CTA owns a 16x16 tile of one slice (blockIdx.x = tile, blockIdx.y strides
 // over slices), each warp a 4x8 sub-tile, so the rotation is uniform per CTA and a warp's taps fall on
-// a compact patch of the volume; the volume (67.6 MB at 256^3) stays resident in the 126 MB L2 and
-// taps are read through the non-coherent L1 path. Volume offsets are 32-bit whenever the volume fits,
-// and the LINEAR path resolves bounds and frequency2index once per axis rather than once per tap.
+// a compact patch of the volume; taps are read through the non-coherent L1 path. Volume offsets are
+// 32-bit whenever the volume fits, and the LINEAR path resolves bounds and frequency2index once per
+// axis rather than once per tap. LINEAR extraction of a complex volume with enough pixels first makes
+// a pair copy of the volume (fp_pairs.cuh) and reads each trilinear cell as four 16-byte loads, four
+// pixels per thread (extract_pairs_kernel).
 //
 // The w-windowed form (wsize > 1) keeps the reference's semantics — outputs are the windowed sum over
 // the w offsets of the z-shifted samples — but sums in registers, in w order, instead of zeroing the

@@ -1,6 +1,6 @@
-// rasterize_central_slices_3d on sm_100a: one thread per slice pixel, trilinear scatter of the pixel
-// into the 2x2x2 voxels around its rotated frequency, plus the Hermitian-plane mirror taps
-// (FourierInsertRasterize, noa/xform/FourierProject.hpp:238-373).
+// rasterize_central_slices_3d on sm_100a: trilinear scatter of every slice pixel into the 2x2x2 voxels
+// around its rotated frequency, plus the Hermitian-plane mirror taps (FourierInsertRasterize,
+// noa/xform/FourierProject.hpp:238-373).
 //
 // The scatter is bound by the L2 reduction rate, which counts one operation per lane whatever its
 // width. So a pixel's value and weight for one voxel travel in ONE reduction: the kernel accumulates
