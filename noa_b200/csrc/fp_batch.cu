@@ -47,8 +47,6 @@ static_assert(sizeof(BatchReq) % 8 == 0, "BatchReq is staged in shared memory as
 
 constexpr int PAIRS_PPT = 4;
 
-// One output pixel (b, y, u) of request `a`: the body of extract_kernel (fp_extract.cu), with 32-bit
-// volume offsets (batches require volumes addressable in 31 bits).
 // PAIRS_PPT output pixels (rows y0, y0 + dy, ...) of column u read through the volume's pair copy:
 // the body of extract_pairs_kernel (fp_extract.cu).
 template<bool OUT_C>
@@ -85,6 +83,8 @@ __device__ __forceinline__ void extract_rows_pairs(const ProjArgs& a, const floa
     }
 }
 
+// One output pixel (b, y, u) of request `a`: the body of extract_kernel (fp_extract.cu), with 32-bit
+// volume offsets (batches require volumes addressable in 31 bits).
 template<int I, bool IN_C, bool OUT_C>
 __device__ __forceinline__ void extract_one(const ProjArgs& a, int64_t b, int y, int u) {
     const Spectrum3 sp{a.vol_d, a.vol_h, a.vol_w, a.in_centered};
@@ -153,9 +153,14 @@ batch_extract_kernel(const BatchReq* __restrict__ reqs, int n_req, int64_t n_ite
     const int lx = (warp % WARPS_X) * VT.wx + lane % VT.wx;
     int staged = -1;   // request held in s_req_words
     int found = 0;     // thread 0: request of the previous item (a CTA's items only increase)
+    // Thread 0 claims the CTA's next item while the current one is processed, so the counter's
+    // round trip is hidden behind the work (the claimed item is always processed by this CTA).
+    long long next = threadIdx.x == 0 ? static_cast<long long>(atomicAdd(counter, 1ull)) : 0;
     for (;;) {
         if (threadIdx.x == 0) {
-            const long long item = static_cast<long long>(atomicAdd(counter, 1ull));
+            const long long item = next;
+            if (item < n_items)
+                next = static_cast<long long>(atomicAdd(counter, 1ull));
             if (item < n_items && found + 1 < n_req && reqs[found + 1].first_item <= item) {
                 int lo = found + 1, hi = n_req - 1;
                 while (lo < hi) {
