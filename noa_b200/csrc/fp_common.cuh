@@ -568,6 +568,11 @@ __device__ __forceinline__ float2 interp_3d(const View3<Idx>& v, const Spectrum3
             if (b0 + START >= lo0 && b0 + END <= hi0 && b1 + START >= lo1 && b1 + END <= hi1 &&
                 b2 + START >= 0 && b2 + END <= hi2) {
                 const Idx x0 = static_cast<Idx>(b2 + START) * v.s2;
+                // With contiguous x and a 16-byte aligned volume, a row of SIZE complex values is read
+                // as SIZE/2 aligned 16-byte loads from the even element at or before its start, plus
+                // one 8-byte load when the start is odd: fewer, wider loads than SIZE 8-byte ones.
+                constexpr bool WIDE = CPLX && SIZE % 2 == 0;
+                const bool wide = WIDE && v.s2 == 1 && (reinterpret_cast<uintptr_t>(v.data) & 15) == 0;
 #pragma unroll (SIZE <= 4 ? SIZE : 1)
                 for (int z = 0; z < SIZE; ++z) {
                     const Idx oz = static_cast<Idx>(frequency2index(sp.centered, b0 + START + z, sp.n0)) * v.s0 + x0;
@@ -576,6 +581,30 @@ __device__ __forceinline__ float2 interp_3d(const View3<Idx>& v, const Spectrum3
                     for (int y = 0; y < SIZE; ++y) {
                         const Idx row = oz + static_cast<Idx>(frequency2index(sp.centered, b1 + START + y, sp.n1)) * v.s1;
                         float2 vy = make_float2(0.f, 0.f);
+                        if constexpr (WIDE) {
+                            if (wide) {
+                                const bool odd = (row & 1) != 0;
+                                const float2* e = static_cast<const float2*>(v.data) + (row - (odd ? 1 : 0));
+                                float4 q[SIZE / 2];
+#pragma unroll
+                                for (int j = 0; j < SIZE / 2; ++j)
+                                    q[j] = __ldg(reinterpret_cast<const float4*>(e) + j);
+                                const float2 last = odd ? __ldg(e + SIZE) : make_float2(0.f, 0.f);
+#pragma unroll
+                                for (int x = 0; x < SIZE; ++x) {
+                                    // element x of the row: element x + odd of the loaded run
+                                    const int i0 = x, i1 = x + 1;
+                                    const float2 even = (i0 & 1) ? make_float2(q[i0 / 2].z, q[i0 / 2].w)
+                                                                 : make_float2(q[i0 / 2].x, q[i0 / 2].y);
+                                    const float2 shifted = i1 == SIZE ? last
+                                        : ((i1 & 1) ? make_float2(q[i1 / 2].z, q[i1 / 2].w)
+                                                    : make_float2(q[i1 / 2].x, q[i1 / 2].y));
+                                    vy = cfma(odd ? shifted : even, w2[x], vy);
+                                }
+                                vz = cfma(vy, w1[y], vz);
+                                continue;
+                            }
+                        }
 #pragma unroll
                         for (int x = 0; x < SIZE; ++x)
                             vy = cfma(view_read<CPLX>(v, row + static_cast<Idx>(x) * v.s2), w2[x], vy);
