@@ -356,9 +356,29 @@ def cpu_baseline(seconds: float) -> dict:
         run(ras, threads)
         done += 2 * batch
     dt = time.perf_counter() - t0
+    # the same sample on one thread, over a quarter of the time
+    done1, t1 = 0, time.perf_counter()
+    while time.perf_counter() - t1 < seconds / 4:
+        run(ext, 1)
+        run(ras, 1)
+        done1 += 2 * batch
+    dt1 = time.perf_counter() - t1
     return {"value": done / dt, "unit": "slices/s", "cores": threads, "kind": kind,
+            "value_1_thread": done1 / dt1, "cpu_model": _cpu_model(),
             "sample": f"{done} slices ({batch}-slice extract + {batch}-slice rasterize batches, 256^3, "
-                      f"{dt:.1f} s, threads={threads}; rasterize runs with noa's per-float omp atomics)"}
+                      f"{dt:.1f} s, threads={threads}; rasterize runs with noa's per-float omp atomics); "
+                      f"1 thread: {done1} slices in {dt1:.1f} s"}
+
+
+def _cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 def run_reference(args) -> None:
