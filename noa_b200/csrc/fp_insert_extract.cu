@@ -1,11 +1,14 @@
 // insert_and_extract_central_slices_3d on sm_100a: every output pixel samples the virtual volume made
 // of the input slices (FourierInsertExtract, noa/xform/FourierProject.hpp:858-977).
 //
-// A CTA owns 256 consecutive pixels of one output slice. The input slices are culled per CTA as in the
-// gather insertion: slice i can only contribute to a pixel whose 3-D frequency g satisfies
-// |n_i . g| < blackman, so with the CTA's bounding sphere (c, rho) of its pixels' frequencies the
-// surviving indices are compacted, in increasing order, into shared memory. Summation order per pixel
-// is therefore the reference's. The w-windowed form sums the w offsets in registers (in w order)
+// A CTA owns a 16x16 tile of one output slice, each warp a 4x8 sub-tile. The input slices are culled
+// twice: slice i can only contribute to a pixel whose 3-D frequency g satisfies |n_i . g| < blackman,
+// and without curvature g is linear in the pixel's 2-D frequency, so n_i . g over a box of pixels is an
+// interval known from two dot products (patch_reaches). The slices whose interval over the CTA's box
+// meets the slab are compacted, in increasing order, into shared memory; each warp re-tests that list
+// against its own box (one candidate per lane) and walks the survivors' ballot in lane order.
+// Summation order per pixel is therefore the reference's (increasing slice index). With an Ewald
+// sphere (curved slices) nothing is culled. The w-windowed form sums the w offsets in registers (in w order)
 // rather than zero-filling and adding atomically; each offset re-samples the virtual volume at the
 // z-shifted frequency.
 #include "fp_args.cuh"
@@ -14,31 +17,41 @@ namespace nb {
 namespace {
 
 constexpr int IE_THREADS = 256;
+constexpr int IE_TILE = 16;  // 16x16 pixels per CTA; warps own 4x8 sub-tiles
 
-__device__ __forceinline__ float3 row0(const XformView& r, int64_t i) {
-    if (r.kind == 3) {
-        float a0 = 1.f, a1 = 0.f, a2 = 0.f;
-        float b0 = 0.f, b1 = 1.f, b2 = 0.f;
-        float c0 = 0.f, c1 = 0.f, c2 = 1.f;
-        rotate(r, i, a0, a1, a2);
-        rotate(r, i, b0, b1, b2);
-        rotate(r, i, c0, c1, c2);
-        return make_float3(a0, b0, c0);
+// A box of 2-D output frequencies: centre and half-extent per axis.
+struct Box2 {
+    float c0, h0, c1, h1;
+    __device__ static Box2 of(float lo0, float hi0, float lo1, float hi1) {
+        return {0.5f * (lo0 + hi0), 0.5f * (hi0 - lo0), 0.5f * (lo1 + hi1), 0.5f * (hi1 - lo1)};
     }
-    const float* m = xform_ptr(r, i, 12);
-    return make_float3(m[0], m[1], m[2]);
+};
+
+// The 3-D frequencies of an output slice's unit 2-D steps (z, y, x).
+struct Patch {
+    float gv0, gv1, gv2, gu0, gu1, gu2;
+};
+
+// Whether input slice i (n = row 0 of its inverse rotation, so that its fz = n . g) can reach
+// |fz| < blackman at a frequency g of the box, shifted along z by `off`: over the box, n . g spans
+// centre +- (|n . Gv| h0 + |n . Gu| h1). The margin covers the rounding of the exact per-pixel test.
+__device__ __forceinline__ bool patch_reaches(const float3 n, const Patch& p, const Box2& box, float off, float fb) {
+    const float al = n.x * p.gv0 + n.y * p.gv1 + n.z * p.gv2;
+    const float be = n.x * p.gu0 + n.y * p.gu1 + n.z * p.gu2;
+    const float centre = al * box.c0 + be * box.c1 + n.x * off;
+    const float half = fabsf(al) * box.h0 + fabsf(be) * box.h1;
+    return fabsf(centre) <= fb + half + 1e-5f * (1.f + fabsf(centre) + half);
 }
 
 template<int I, bool IN_C, bool OUT_C>
 __global__ void __launch_bounds__(IE_THREADS)
-insert_extract_kernel(const __grid_constant__ ProjArgs a, int tiles_per_slice, int64_t n_tiles) {
+insert_extract_kernel(const __grid_constant__ ProjArgs a, int ntx, int tiles_per_slice, int64_t n_tiles) {
     __shared__ int s_list[IE_THREADS];
     __shared__ int s_warp_count[IE_THREADS / 32];
     __shared__ int s_count;
-    __shared__ float s_box[6][IE_THREADS / 32];
+    __shared__ float s_box[4][IE_THREADS / 32];
 
     const int wp = a.slice_w / 2 + 1;
-    const int plane = a.slice_h * wp;
     const Spectrum2 sp{a.in_h, a.in_w_, a.in_centered, a.in_slice_narrow != 0};
     const bool has_out_w = a.out_w.present;
     const bool has_in_w = a.in_w.present;
@@ -46,49 +59,52 @@ insert_extract_kernel(const __grid_constant__ ProjArgs a, int tiles_per_slice, i
 
     for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
         const int64_t b = tile / tiles_per_slice;
-        const int p = static_cast<int>(tile - b * tiles_per_slice) * IE_THREADS + tid;
-        const bool valid = p < plane;
-        const int y = valid ? p / wp : 0;
-        const int u = valid ? p - y * wp : 0;
+        const int t = static_cast<int>(tile - b * tiles_per_slice);
+        const int ty = t / ntx, tx = t - ty * ntx;
+        const int py = ty * IE_TILE + (warp >> 1) * 4 + (lane >> 3);
+        const int pu = tx * IE_TILE + (warp & 1) * 8 + (lane & 7);
+        const bool valid = py < a.slice_h && pu < wp;
+        const int y = valid ? py : 0;
+        const int u = valid ? pu : 0;
         const int v = index2frequency(a.out_centered, y, a.slice_h);
+        const float pf0 = div(static_cast<float>(v), a.f_slice0), pf1 = div(static_cast<float>(u), a.f_slice1);
         float gz, gy, gx;
-        slice2grid(div(static_cast<float>(v), a.f_slice0), div(static_cast<float>(u), a.f_slice1),
-                   a.scale2, a.rot2, b, a.ews, gz, gy, gx);
+        slice2grid(pf0, pf1, a.scale2, a.rot2, b, a.ews, gz, gy, gx);
 
-        // The frequencies this pixel samples: g, plus the z offsets of the w window.
-        const float wz_lo = a.wsize > 1 ? div(static_cast<float>(0 - a.wsize / 2), a.vz) : 0.f;
-        const float wz_hi = a.wsize > 1 ? div(static_cast<float>(a.wsize - 1 - a.wsize / 2), a.vz) : 0.f;
-
-        // CTA bounding box of the sampled frequencies (valid pixels only).
-        float bmin[3] = {valid ? add(gz, wz_lo) : 3.4e38f, valid ? gy : 3.4e38f, valid ? gx : 3.4e38f};
-        float bmax[3] = {valid ? add(gz, wz_hi) : -3.4e38f, valid ? gy : -3.4e38f, valid ? gx : -3.4e38f};
+        // Without curvature a pixel's frequency is linear in its 2-D frequency: g = pf0 Gv + pf1 Gu.
+        // Over a box of 2-D frequencies, n . g therefore spans an interval whose centre and half-width
+        // follow from n . Gv and n . Gu (patch_reaches); the boxes are the warp's and the CTA's.
+        Patch patch;
+        slice2grid(1.f, 0.f, a.scale2, a.rot2, b, a.ews, patch.gv0, patch.gv1, patch.gv2);
+        slice2grid(0.f, 1.f, a.scale2, a.rot2, b, a.ews, patch.gu0, patch.gu1, patch.gu2);
+        float bmin[2] = {valid ? pf0 : 3.4e38f, valid ? pf1 : 3.4e38f};
+        float bmax[2] = {valid ? pf0 : -3.4e38f, valid ? pf1 : -3.4e38f};
 #pragma unroll
-        for (int ax = 0; ax < 3; ++ax) {
+        for (int ax = 0; ax < 2; ++ax) {
             for (int o = 16; o > 0; o >>= 1) {
                 bmin[ax] = fminf(bmin[ax], __shfl_xor_sync(0xffffffffu, bmin[ax], o));
                 bmax[ax] = fmaxf(bmax[ax], __shfl_xor_sync(0xffffffffu, bmax[ax], o));
             }
             if (lane == 0) {
                 s_box[ax][warp] = bmin[ax];
-                s_box[3 + ax][warp] = bmax[ax];
+                s_box[2 + ax][warp] = bmax[ax];
             }
         }
+        // After the butterfly every lane holds its warp's box.
+        const bool warp_valid = __any_sync(0xffffffffu, valid);
+        const Box2 wbox = Box2::of(bmin[0], bmax[0], bmin[1], bmax[1]);
         __syncthreads();
-        float lo[3], hi[3];
+        float lo[2], hi[2];
 #pragma unroll
-        for (int ax = 0; ax < 3; ++ax) {
+        for (int ax = 0; ax < 2; ++ax) {
             lo[ax] = 3.4e38f;
             hi[ax] = -3.4e38f;
             for (int w = 0; w < IE_THREADS / 32; ++w) {
                 lo[ax] = fminf(lo[ax], s_box[ax][w]);
-                hi[ax] = fmaxf(hi[ax], s_box[3 + ax][w]);
+                hi[ax] = fmaxf(hi[ax], s_box[2 + ax][w]);
             }
         }
-        const float c0 = 0.5f * (lo[0] + hi[0]), c1 = 0.5f * (lo[1] + hi[1]), c2 = 0.5f * (lo[2] + hi[2]);
-        const float h0 = 0.5f * (hi[0] - lo[0]), h1 = 0.5f * (hi[1] - lo[1]), h2 = 0.5f * (hi[2] - lo[2]);
-        const float rho = sqrtf(h0 * h0 + h1 * h1 + h2 * h2);
-        const float cn = sqrtf(c0 * c0 + c1 * c1 + c2 * c2);
-        const float margin = 1e-5f * (cn + rho + 1.f);
+        const Box2 cbox = Box2::of(lo[0], hi[0], lo[1], hi[1]);
         const bool cull = !a.ews.on;
 
         // Accumulators: one (value, weight) per w offset would be needed for the windowed form, so
@@ -109,16 +125,8 @@ insert_extract_kernel(const __grid_constant__ ProjArgs a, int tiles_per_slice, i
             for (int64_t chunk = 0; chunk < a.n_in; chunk += IE_THREADS) {
                 const int64_t i = chunk + tid;
                 bool keep = false;
-                if (i < a.n_in) {
-                    if (cull) {
-                        const float3 n = row0(a.rot, i);
-                        const float nn = sqrtf(n.x * n.x + n.y * n.y + n.z * n.z);
-                        const float d = fabsf(n.x * c0 + n.y * c1 + n.z * c2);
-                        keep = d <= a.fb + nn * rho + margin * (1.f + nn);
-                    } else {
-                        keep = true;
-                    }
-                }
+                if (i < a.n_in)
+                    keep = !cull || patch_reaches(rotation_row0(a.rot, i), patch, cbox, off, a.fb);
                 const unsigned ballot = __ballot_sync(0xffffffffu, keep);
                 if (lane == 0)
                     s_warp_count[warp] = __popc(ballot);
@@ -132,9 +140,19 @@ insert_extract_kernel(const __grid_constant__ ProjArgs a, int tiles_per_slice, i
                     s_count = base + __popc(ballot);
                 __syncthreads();
                 const int count = s_count;
-                if (in_cut) {
-                    for (int k = 0; k < count; ++k) {
-                        const int64_t si = chunk + s_list[k];
+                // Warp-uniform loops: the list, the ballot and warp_valid are the same in every lane.
+                for (int g = 0; warp_valid && g < count; g += 32) {
+                    const int k = g + lane;
+                    const bool wkeep = k < count &&
+                                       (!cull || patch_reaches(rotation_row0(a.rot, chunk + s_list[k]), patch, wbox,
+                                                               off, a.fb));
+                    unsigned todo = __ballot_sync(0xffffffffu, wkeep);
+                    while (todo) {
+                        const int j = __ffs(todo) - 1;
+                        todo &= todo - 1u;
+                        if (!in_cut)
+                            continue;
+                        const int64_t si = chunk + s_list[g + j];
                         float f0, f1;
                         const float fz = grid2slice(sz, gy, gx, a.scale, a.rot, si, a.ews, f0, f1);
                         if (fabsf(fz) < a.fb) {
@@ -208,14 +226,14 @@ insert_extract_kernel(const __grid_constant__ ProjArgs a, int tiles_per_slice, i
 template<int I, bool IN_C, bool OUT_C>
 cudaError_t launch_typed(const ProjArgs& a, cudaStream_t stream) {
     const int wp = a.slice_w / 2 + 1;
-    const int plane = a.slice_h * wp;
-    const int tiles_per_slice = (plane + IE_THREADS - 1) / IE_THREADS;
+    const int ntx = (wp + IE_TILE - 1) / IE_TILE, nty = (a.slice_h + IE_TILE - 1) / IE_TILE;
+    const int tiles_per_slice = ntx * nty;
     const int64_t n_tiles = static_cast<int64_t>(tiles_per_slice) * a.n_slices;
     if (n_tiles == 0)
         return cudaSuccess;
     const int64_t max_grid = static_cast<int64_t>(sm_count()) * 8 * 16;
     const int grid = static_cast<int>(n_tiles < max_grid ? n_tiles : max_grid);
-    insert_extract_kernel<I, IN_C, OUT_C><<<grid, IE_THREADS, 0, stream>>>(a, tiles_per_slice, n_tiles);
+    insert_extract_kernel<I, IN_C, OUT_C><<<grid, IE_THREADS, 0, stream>>>(a, ntx, tiles_per_slice, n_tiles);
     return cudaGetLastError();
 }
 
