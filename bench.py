@@ -34,6 +34,7 @@ N = 256
 SLICES = 4096
 BFACTOR = 100.0
 L2_FLUSH_BYTES = 256 << 20      # > 126 MB L2
+REFERENCE_SECONDS = 150.0       # bound on the timed steps of the reference arm
 E2E_CHUNKS = 8                  # slice chunks of the end-to-end step (overlapped copies)
 
 
@@ -342,18 +343,31 @@ def _cpu_impl():
     return "port", (lambda call, thr: lib.run(call, thr))
 
 
+# noa's CPU backend gives each thread at least 2^20 indices (runtime/Iwise.hpp:34-35) and runs a call
+# serially below that, so a sample must hold threads x 2^20 pixels for noa to use every host thread.
+NOA_INDICES_PER_THREAD = 1 << 20
+
+
+def cpu_sample_slices(threads: int) -> int:
+    """Slices per CPU call: enough pixels for noa to spread a call over `threads`, a multiple of 32."""
+    need = -(-threads * NOA_INDICES_PER_THREAD // (N * (N // 2 + 1)))
+    return max(32, -(-need // 32) * 32)
+
+
 def cpu_baseline(seconds: float) -> dict:
     """noa's CPU path timed on this host's cores over a bounded sample of the workload."""
     kind, run = _cpu_impl()
     threads = os.cpu_count() or 1
-    batch = 32
+    batch = cpu_sample_slices(threads)
     ext, ras = _cpu_sample(batch)
     run(ext, threads)           # warm-up
     run(ras, threads)
-    done, t0 = 0, time.perf_counter()
-    while time.perf_counter() - t0 < seconds:
+    done, t0, iters = 0, time.perf_counter(), []
+    while time.perf_counter() - t0 < seconds or len(iters) < 5:
+        ti = time.perf_counter()
         run(ext, threads)
         run(ras, threads)
+        iters.append(time.perf_counter() - ti)
         done += 2 * batch
     dt = time.perf_counter() - t0
     # the same sample on one thread, over a quarter of the time
@@ -363,11 +377,13 @@ def cpu_baseline(seconds: float) -> dict:
         run(ras, 1)
         done1 += 2 * batch
     dt1 = time.perf_counter() - t1
-    return {"value": done / dt, "unit": "slices/s", "cores": threads, "kind": kind,
+    return {"value": 2 * batch / statistics.median(iters), "unit": "slices/s", "cores": threads, "kind": kind,
             "value_1_thread": done1 / dt1, "cpu_model": _cpu_model(),
-            "sample": f"{done} slices ({batch}-slice extract + {batch}-slice rasterize batches, 256^3, "
-                      f"{dt:.1f} s, threads={threads}; rasterize runs with noa's per-float omp atomics); "
-                      f"1 thread: {done1} slices in {dt1:.1f} s"}
+            "sample": f"median of {len(iters)} repetitions; "
+                      f"{done} slices ({batch}-slice extract + {batch}-slice rasterize calls, 256^3, "
+                      f"{dt:.1f} s, threads={threads}; {batch} slices per call so that noa spreads each call "
+                      f"over all threads (it gives a thread at least 2^20 pixels); rasterize runs with noa's "
+                      f"per-float omp atomics); 1 thread: {done1} slices in {dt1:.1f} s"}
 
 
 def _cpu_model() -> str:
@@ -387,13 +403,18 @@ def run_reference(args) -> None:
         return
     kind, run = _cpu_impl()
     threads = os.cpu_count() or 1
-    batch = args.ref_batch
+    batch = args.ref_batch or cpu_sample_slices(threads)
     ext, ras = _cpu_sample(batch)
-    for _ in range(args.warmup):
+    t0 = time.perf_counter()
+    for _ in range(max(args.warmup, 1)):
         run(ext, threads)
         run(ras, threads)
+    per_step = (time.perf_counter() - t0) / max(args.warmup, 1)
+    # K steps of a sample large enough for noa's threading can take long: keep the run within about
+    # three minutes, and report the number of steps timed.
+    steps = min(args.steps, max(3, int(REFERENCE_SECONDS / max(per_step, 1e-6))))
     times = []
-    for _ in range(args.steps):
+    for _ in range(steps):
         t0 = time.perf_counter()
         run(ext, threads)
         run(ras, threads)
@@ -404,12 +425,14 @@ def run_reference(args) -> None:
         "impl": "reference",
         "metric": "slices/sec extract & insert at 256^3",
         "value": value, "unit": "slices/s", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": step * 1e3, "higher_is_better": True,
+        "steps": steps, "steps_requested": args.steps, "warmup": max(args.warmup, 1), "ms_per_step": step * 1e3,
+        "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded; no dataset)",
         "config": {"workload": "extract + rasterize slices of 256x129 c64, 256^3 rfft volume (+f32 weights)",
                    "slices_per_op_per_step": batch, "remaps": ["hc2h", "h2hc"], "interp": "linear"},
         "cpu_baseline": {"value": value, "unit": "slices/s", "cores": threads, "kind": kind,
-                         "sample": f"{batch}-slice extract + {batch}-slice rasterize per step, {threads} threads"},
+                         "sample": f"{batch}-slice extract + {batch}-slice rasterize per step, {threads} threads "
+                                   f"({batch} slices per call so that noa spreads each call over all threads)"},
         "e2e": {"value": value, "unit": "slices/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
@@ -604,10 +627,17 @@ def _insert_extract_cpu_baseline(h_in, h_rot_in, h_rot_out, n: int, total: int) 
     t0 = time.perf_counter()
     run(c, threads)
     dt = time.perf_counter() - t0
-    return ({"value": k / dt, "unit": "slices/s", "cores": threads, "kind": kind,
-             "sample": f"{k} of the {total} output slices from all {b} input slices in {dt:.1f} s, "
-                       f"threads={threads}; noa's loop visits every (output pixel, input slice) pair, so its "
-                       f"time is linear in the output slice count and the rate extrapolates to the full job"},
+    # noa gives a thread at least 2^20 output pixels, so a call over k < 32 output slices of 256x129 runs
+    # on one thread, and any call of >= 32 slices takes as long as one thread's 32 slices (over a minute
+    # here). The sample is therefore serial; its rate times the host's threads bounds noa's parallel rate.
+    used = max(1, min(threads, (k * n * wp) // NOA_INDICES_PER_THREAD))
+    return ({"value": k / dt, "unit": "slices/s", "cores": used, "kind": kind,
+             "value_all_threads_bound": k / dt * threads / used, "host_threads": threads,
+             "sample": f"{k} of the {total} output slices from all {b} input slices in {dt:.1f} s; noa ran it "
+                       f"on {used} thread(s) (it gives a thread at least 2^20 output pixels); its loop visits "
+                       f"every (output pixel, input slice) pair, so its time is linear in the output slice "
+                       f"count and the rate extrapolates to the full job; value_all_threads_bound assumes "
+                       f"perfect scaling over the {threads} host threads"},
             c.out.astype(np.complex128), c.out_w.astype(np.float64))
 
 
@@ -620,7 +650,8 @@ def main() -> None:
     p.add_argument("--e2e-steps", type=int, default=5)
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--ref-batch", type=int, default=32)
+    p.add_argument("--ref-batch", type=int, default=None,
+                   help="slices per CPU call of the reference arm (default: enough for noa to use every thread)")
     p.add_argument("--n", type=int, default=None, help="box size (default 256, or 512 for insert_512)")
     p.add_argument("--slices", type=int, default=None, help="slices per op per step")
     p.add_argument("--workload", choices=["extract_insert_256", "insert_512", "insert_extract_256"],
