@@ -641,6 +641,70 @@ def _insert_extract_cpu_baseline(h_in, h_rot_in, h_rot_out, n: int, total: int) 
             c.out.astype(np.complex128), c.out_w.astype(np.float64))
 
 
+# ---------------------------------------------------------------------------------------------------
+# Fourth workload: batched uneven LANCZOS8 extraction (persistent kernel in a CUDA graph).
+# ---------------------------------------------------------------------------------------------------
+def run_batched(args) -> None:
+    """12,000 LANCZOS8 extractions over 12 resident volumes of 128-384 (noa_b200.workloads.batched):
+    the graph-captured persistent launch against per-call launches, with noa's CPU path beside it."""
+    import torch
+    from noa_b200 import workloads
+    wargs = argparse.Namespace(seed=0, total=args.slices, interp="lanczos8", no_autotune=False,
+                               steps=args.steps, warmup=max(args.warmup, 3))
+    r = workloads.batched(wargs)
+    boxes = [128, 192, 256, 384] * 3
+    counts = r["config"]["slices_per_volume"]
+    alg = sum(8 * n * n * (n // 2 + 1) + c * (8 * n * (n // 2 + 1) + 48) for n, c in zip(boxes, counts))
+    ms = r["batched"]["ms"]
+    peaks = measured_peaks()
+    achieved = alg / (ms * 1e-3) / 1e9
+    line = {
+        "metric": "slices/sec batched uneven LANCZOS8 extraction", "value": r["batched"]["value"],
+        "unit": "slices/s", "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded; no dataset)",
+        "config": {"workload": f"{sum(counts)} LANCZOS8 extractions (hc2h, cutoff 0.5) over 12 volumes of "
+                               f"128-384 in one graph-captured persistent launch", **r["config"]},
+        "per_call": r["per_call"], "speedup_batched_vs_per_call": r["speedup_batched_vs_per_call"],
+        "launch": r["batched"]["launch"],
+        "roofline": {"bound": "hbm", "kernel": "batch_extract_kernel", "achieved": achieved,
+                     "peak": peaks["hbm_gbs"], "peak_source": peaks["source"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"], "algorithmic_bytes": alg, "traffic": None},
+        "gpu_launches": args.steps,
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = _batched_cpu_baseline(boxes, counts)
+    print(json.dumps(line), flush=True)
+
+
+def _batched_cpu_baseline(boxes, counts, pixels_per_box: int = 200_000) -> dict:
+    """noa's CPU LANCZOS8 extraction timed per box size on a serial sample (fewer than 2^20 pixels, so
+    noa runs it on one thread), then the full job's time as the sum over volumes of count x time per
+    slice of its box."""
+    from noa_b200 import synthetic
+    from oracle.oracle import Call, INTERPS
+    kind, run = _cpu_impl()
+    per_slice, notes = {}, []
+    for n in sorted(set(boxes)):
+        wp = n // 2 + 1
+        k = max(1, pixels_per_box // (n * wp))
+        vol = synthetic.make_volume(n, seed=n)
+        c = Call(func="extract", remap="hc2h", inp=vol, in_shape=(1, n, n, n),
+                 out=np.zeros((k, 1, n, wp), np.complex64), out_shape=(k, 1, n, n),
+                 rot=synthetic.random_rotations(k, seed=n + 1), interp=INTERPS["lanczos8"])
+        t0 = time.perf_counter()
+        run(c, 1)
+        per_slice[n] = (time.perf_counter() - t0) / k
+        notes.append(f"{n}: {k} slices, {per_slice[n] * 1e3:.0f} ms/slice")
+    job = sum(c * per_slice[n] for n, c in zip(boxes, counts))
+    threads = os.cpu_count() or 1
+    return {"value": sum(counts) / job, "unit": "slices/s", "cores": 1, "kind": kind,
+            "value_all_threads_bound": sum(counts) / job * threads, "host_threads": threads,
+            "sample": "per box, one serial call (noa runs calls under 2^20 pixels on one thread): "
+                      + "; ".join(notes) + f"; job time = sum of count x time per slice = {job:.0f} s; "
+                      f"value_all_threads_bound assumes perfect scaling over {threads} threads"}
+
+
 def main() -> None:
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -654,15 +718,21 @@ def main() -> None:
                    help="slices per CPU call of the reference arm (default: enough for noa to use every thread)")
     p.add_argument("--n", type=int, default=None, help="box size (default 256, or 512 for insert_512)")
     p.add_argument("--slices", type=int, default=None, help="slices per op per step")
-    p.add_argument("--workload", choices=["extract_insert_256", "insert_512", "insert_extract_256"],
+    p.add_argument("--workload", choices=["extract_insert_256", "insert_512", "insert_extract_256", "batched"],
                    default="extract_insert_256",
                    help="insert_512: the 512^3 x 20,000 windowed-sinc insertion, gather vs scatter form; "
-                        "insert_extract_256: insert_and_extract_central_slices_3d, 4096 in, 256 out")
+                        "insert_extract_256: insert_and_extract_central_slices_3d, 4096 in, 256 out; "
+                        "batched: 12,000 LANCZOS8 extractions over 12 volumes in one persistent launch")
     p.add_argument("--out-slices", type=int, default=256, help="insert_extract_256: output slices")
     p.add_argument("--ref-slices", type=int, default=None,
                    help="slices of the CPU reference sample (insert_512: 64 input, insert_extract_256: 2 output)")
     args = p.parse_args()
     global N, SLICES
+    if args.workload == "batched":
+        args.slices = args.slices or 12000
+        args.steps = min(args.steps, 5)
+        run_batched(args)
+        return
     if args.workload == "insert_extract_256":
         args.n = args.n or 256
         args.slices = args.slices or 4096
