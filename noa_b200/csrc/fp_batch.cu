@@ -3,9 +3,11 @@
 //
 // Work decomposition: every request is cut into (slice, tile) items, a tile being TY x TX pixels of
 // one output slice (4 TY x TX for a request read through its volume's pair copy, 4 rows per thread).
-// Items are numbered request after request; a device counter hands them out, one per CTA at a time
-// (atomicAdd), so uneven requests balance themselves across the SMs without a per-request launch. A
-// CTA stages the descriptor of its current request in shared memory. Each item runs the per-pixel
+// Items are numbered request after request; a device counter hands them out in chunks of
+// consecutive items (atomicAdd; about 64 claims per CTA over a launch, at most 64 items per claim), so
+// uneven requests balance themselves across the SMs without a per-request launch and cheap items do
+// not queue on the counter. A CTA stages the descriptor of its current request in shared memory and
+// crosses a barrier only when its request changes. Each item runs the per-pixel
 // code of nb_extract_central_slices_3d (extract_one restates the generic kernel body for one pixel,
 // extract_rows_pairs the pair-copy kernel body for 4 rows), so results are bit-identical to the
 // per-call entry point.
@@ -144,24 +146,40 @@ batch_extract_kernel(const BatchReq* __restrict__ reqs, int n_req, int64_t n_ite
     constexpr Variant VT = VARIANTS[V];
     constexpr int WORDS = sizeof(BatchReq) / 8;
     __shared__ unsigned long long s_req_words[WORDS];  // the current request, staged once per change
-    __shared__ long long s_item;
-    __shared__ int s_req;
     const BatchReq& R = *reinterpret_cast<const BatchReq*>(s_req_words);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     constexpr int WARPS_X = VT.tx / VT.wx;
     const int ly = (warp / WARPS_X) * VT.wy + lane / VT.wx;
     const int lx = (warp % WARPS_X) * VT.wx + lane % VT.wx;
     int staged = -1;   // request held in s_req_words
-    int found = 0;     // thread 0: request of the previous item (a CTA's items only increase)
-    // Thread 0 claims the CTA's next item while the current one is processed, so the counter's
-    // round trip is hidden behind the work (the claimed item is always processed by this CTA).
-    long long next = threadIdx.x == 0 ? static_cast<long long>(atomicAdd(counter, 1ull)) : 0;
-    for (;;) {
+    int found = 0;     // request of the last item (a CTA's items only increase)
+    // Items are claimed in chunks of consecutive items, ~64 claims per CTA over the launch (at most 64
+    // items per claim), so cheap items do not queue on the counter. Thread 0 claims the next chunk
+    // while the current one is processed, so the counter's round trip is hidden behind the work.
+    const long long per_cta = n_items / (static_cast<long long>(gridDim.x) * 64);
+    const long long chunk = per_cta < 1 ? 1 : (per_cta > 64 ? 64 : per_cta);
+    __shared__ long long s_chunk[2];
+    long long next = threadIdx.x == 0 ? static_cast<long long>(atomicAdd(counter, static_cast<unsigned long long>(chunk))) : 0;
+    for (int round = 0;; ++round) {
         if (threadIdx.x == 0) {
-            const long long item = next;
-            if (item < n_items)
-                next = static_cast<long long>(atomicAdd(counter, 1ull));
-            if (item < n_items && found + 1 < n_req && reqs[found + 1].first_item <= item) {
+            s_chunk[round & 1] = next;
+            if (next < n_items)
+                next = static_cast<long long>(atomicAdd(counter, static_cast<unsigned long long>(chunk)));
+        }
+        __syncthreads();
+        // Double-buffered: thread 0 writes the other slot next round, after at least one more barrier.
+        const long long c0 = s_chunk[round & 1];
+        if (c0 >= n_items)
+            break;
+        const long long c1 = c0 + chunk < n_items ? c0 + chunk : n_items;
+        // (slice, tile row, tile column) of the item: divided out once per chunk or request, then
+        // advanced item by item (consecutive items walk a slice's tiles row-major).
+        int64_t b = 0;
+        int ty = 0, tx = 0, nty = 1;
+        bool fresh = true;
+        for (long long item = c0; item < c1; ++item) {
+            // Every thread finds the item's request the same way (uniform), from the previous one.
+            if (found + 1 < n_req && reqs[found + 1].first_item <= item) {
                 int lo = found + 1, hi = n_req - 1;
                 while (lo < hi) {
                     const int mid = (lo + hi + 1) / 2;
@@ -172,36 +190,45 @@ batch_extract_kernel(const BatchReq* __restrict__ reqs, int n_req, int64_t n_ite
                 }
                 found = lo;
             }
-            s_item = item;
-            s_req = found;
-        }
-        __syncthreads();
-        const long long item = s_item;
-        const int r = s_req;
-        if (item >= n_items)
-            break;
-        if (r != staged) {
-            const auto* src = reinterpret_cast<const unsigned long long*>(reqs + r);
-            for (int i = threadIdx.x; i < WORDS; i += blockDim.x)
-                s_req_words[i] = src[i];
-            staged = r;
-        }
-        __syncthreads();
-        const int64_t local = item - R.first_item;
-        const int64_t b = local / R.tiles_per_slice;
-        const int tile = static_cast<int>(local - b * R.tiles_per_slice);
-        const int u = (tile % R.ntx) * VT.tx + lx;
-        if (u < R.a.slice_w / 2 + 1) {
-            if constexpr (I == I_LINEAR && IN_C) {
-                if (PAIRS_ONLY || R.pairs) {
-                    extract_rows_pairs<OUT_C>(R.a, R.pairs, b, (tile / R.ntx) * (VT.ty * PAIRS_PPT) + ly, VT.ty, u);
-                    continue;
+            if (found != staged) {
+                __syncthreads();  // nobody still reads the previous descriptor
+                const auto* src = reinterpret_cast<const unsigned long long*>(reqs + found);
+                for (int i = threadIdx.x; i < WORDS; i += blockDim.x)
+                    s_req_words[i] = src[i];
+                staged = found;
+                fresh = true;
+                __syncthreads();
+            }
+            if (fresh) {
+                const int64_t local = item - R.first_item;
+                b = local / R.tiles_per_slice;
+                const int tile = static_cast<int>(local - b * R.tiles_per_slice);
+                ty = tile / R.ntx;
+                tx = tile - ty * R.ntx;
+                nty = R.tiles_per_slice / R.ntx;
+                fresh = false;
+            }
+            const int u = tx * VT.tx + lx;
+            if (u < R.a.slice_w / 2 + 1) {
+                bool done = false;
+                if constexpr (I == I_LINEAR && IN_C) {
+                    if (PAIRS_ONLY || R.pairs) {
+                        extract_rows_pairs<OUT_C>(R.a, R.pairs, b, ty * (VT.ty * PAIRS_PPT) + ly, VT.ty, u);
+                        done = true;
+                    }
+                }
+                if constexpr (!PAIRS_ONLY) {
+                    const int y = ty * VT.ty + ly;
+                    if (!done && y < R.a.slice_h)
+                        extract_one<I, IN_C, OUT_C>(R.a, b, y, u);
                 }
             }
-            if constexpr (!PAIRS_ONLY) {
-                const int y = (tile / R.ntx) * VT.ty + ly;
-                if (y < R.a.slice_h)
-                    extract_one<I, IN_C, OUT_C>(R.a, b, y, u);
+            if (++tx == R.ntx) {
+                tx = 0;
+                if (++ty == nty) {
+                    ty = 0;
+                    ++b;
+                }
             }
         }
     }

@@ -33,25 +33,31 @@ def _timer(fn, reps: int, flush) -> list[float]:
 
 
 def batched(args) -> dict:
-    """12,000 LANCZOS8 extractions over 12 resident volumes (3 each of 128, 192, 256, 384; hc2h,
-    cutoff 0.5), slice counts lognormal (median 1000, sigma 0.5, seeded) rescaled to 12,000."""
+    """12,000 extractions (LANCZOS8 by default) over 12 resident volumes (3 each of 128, 192, 256, 384;
+    hc2h, cutoff 0.5), in `requests` requests (default 12, one per volume; request i reads volume
+    i mod 12) whose slice counts are lognormal (median 1000, sigma 0.5, seeded) rescaled to 12,000.
+    Legs: every request through the per-call API, the captured persistent launch (ExtractBatch) and,
+    for LINEAR, one launch over resident pair copies of the volumes (extract_batch_launch), the form
+    the serving loop uses."""
     import torch
     from . import fourier_project as fp
     from . import synthetic
-    from .batch import ExtractBatch, ExtractRequest
+    from .batch import ExtractBatch, ExtractRequest, extract_batch_launch, volume_pairs
     torch.cuda.set_device(0)
     rng = np.random.default_rng(args.seed)
     boxes = [128, 192, 256, 384] * 3
-    counts = rng.lognormal(mean=np.log(1000), sigma=0.5, size=len(boxes))
+    n_req = getattr(args, "requests", None) or len(boxes)
+    counts = rng.lognormal(mean=np.log(1000), sigma=0.5, size=n_req)
     counts = np.maximum(1, np.round(counts / counts.sum() * args.total)).astype(int)
     counts[-1] += args.total - counts.sum()
+    vols = [torch.from_numpy(synthetic.make_volume(n, seed=args.seed + i)).cuda() for i, n in enumerate(boxes)]
     reqs = []
-    for i, (n, c) in enumerate(zip(boxes, counts)):
-        vol = torch.from_numpy(synthetic.make_volume(n, seed=args.seed + i)).cuda()
+    for i, c in enumerate(counts):
+        n = boxes[i % len(boxes)]
         rot = fp.pack_rotations(torch.from_numpy(synthetic.random_rotations(int(c), seed=args.seed + 100 + i)).cuda())
         out = torch.empty((int(c), 1, n, n // 2 + 1), dtype=torch.complex64, device="cuda")
-        reqs.append(ExtractRequest(volume=vol, volume_shape=(1, n, n, n), slice=out, slice_shape=(int(c), 1, n, n),
-                                   fwd_rotation=rot))
+        reqs.append(ExtractRequest(volume=vols[i % len(boxes)], volume_shape=(1, n, n, n), slice=out,
+                                   slice_shape=(int(c), 1, n, n), fwd_rotation=rot))
     flush_buf = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
 
     def flush():
@@ -70,11 +76,26 @@ def batched(args) -> dict:
     t_call = _timer(per_call, args.steps, flush)
     t_batch = _timer(batch.run, args.steps, flush)
     total = int(counts.sum())
+    resident = None
+    if args.interp == "linear":
+        pairs_v = [volume_pairs(v, (1, n, n, n)) for v, n in zip(vols, boxes)]
+        pairs = [pairs_v[i % len(boxes)] for i in range(len(reqs))]
+
+        def launch():
+            extract_batch_launch("hc2h", reqs, pairs, interp=args.interp)
+
+        for _ in range(args.warmup):
+            launch()
+        torch.cuda.synchronize()
+        t_res = _timer(launch, args.steps, flush)
+        resident = {"value": total / (statistics.median(t_res) * 1e-3), "ms": statistics.median(t_res),
+                    "speedup_vs_per_call": statistics.median(t_call) / statistics.median(t_res)}
     return {
         "workload": "batched uneven extraction",
-        "config": {"boxes": sorted(set(boxes)), "volumes": len(boxes), "slices": total,
-                   "slices_per_volume": [int(c) for c in counts], "interp": args.interp, "remap": "hc2h",
-                   "cutoff": 0.5, "l2": "flushed before each repetition"},
+        "config": {"boxes": sorted(set(boxes)), "volumes": len(boxes), "requests": len(reqs), "slices": total,
+                   "slices_per_volume" if len(reqs) == len(boxes) else "slices_per_request": [int(c) for c in counts],
+                   "interp": args.interp, "remap": "hc2h", "cutoff": 0.5, "l2": "flushed before each repetition"},
+        "resident_pairs_launch": resident,
         "unit": "slices/s",
         "batched": {"value": total / (statistics.median(t_batch) * 1e-3), "ms": statistics.median(t_batch),
                     "launch": batch.info()},
@@ -215,6 +236,7 @@ def main() -> None:
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--seed", type=int, default=0)
     p.add_argument("--total", type=int, default=12000)
+    p.add_argument("--requests", type=int, default=None, help="batched: requests over the 12 volumes (default 12)")
     p.add_argument("--interp", default="lanczos8")
     p.add_argument("--no-autotune", action="store_true")
     p.add_argument("--volumes", type=int, default=32)
