@@ -78,3 +78,61 @@ def test_batch_rejects_mixed_types():
     reqs[0].slice = torch.zeros((count, 1, n, n // 2 + 1), dtype=torch.float32, device="cuda")
     with pytest.raises(fp.NoaB200Error):
         ExtractBatch("hc2h", reqs, interp="linear", autotune=False)
+
+
+def _large_requests(spec, seed=0):
+    import torch
+    from noa_b200 import synthetic
+    from noa_b200.batch import ExtractRequest
+    reqs, vols = [], {}
+    for i, (n, count) in enumerate(spec):
+        if n not in vols:
+            vols[n] = torch.from_numpy(synthetic.make_volume(n, seed=seed + n)).cuda()
+        rot = torch.from_numpy(synthetic.random_rotations(count, seed=seed + 70 + i)).cuda()
+        out = torch.full((count, 1, n, n // 2 + 1), 7, dtype=torch.complex64, device="cuda")
+        reqs.append(ExtractRequest(volume=vols[n], volume_shape=(1, n, n, n), slice=out,
+                                   slice_shape=(count, 1, n, n), fwd_rotation=rot))
+    return reqs, vols
+
+
+def _per_call_equal(reqs, interp):
+    import torch
+    from noa_b200 import fourier_project as fp
+    for r in reqs:
+        count, n = r.slice_shape[0], r.slice_shape[2]
+        ref = torch.zeros((count, 1, n, n // 2 + 1), dtype=torch.complex64, device="cuda")
+        fp.extract_central_slices_3d("hc2h", r.volume, None, r.volume_shape, ref, None, r.slice_shape, None,
+                                     r.fwd_rotation, interp=interp)
+        torch.cuda.synchronize()
+        assert torch.equal(r.slice, ref)
+
+
+# Enough items that the persistent kernel claims several consecutive items at a time (more than
+# 2 x 64 per CTA), so runs cross slice and request boundaries inside one claim.
+LARGE = [(128, 1500), (96, 2000), (112, 1201), (64, 903), (128, 700), (80, 1000), (112, 37)]
+
+
+@pytest.mark.parametrize("interp", ["linear", "cubic"])
+def test_batch_long_claims_match_per_call(interp, tmp_path, monkeypatch):
+    import torch
+    from noa_b200.batch import ExtractBatch
+    monkeypatch.setenv("NB_AUTOTUNE_CACHE", str(tmp_path / "autotune.txt"))
+    reqs, _ = _large_requests(LARGE)
+    batch = ExtractBatch("hc2h", reqs, interp=interp, autotune=False)
+    info = batch.info()
+    assert info["n_items"] // (info["grid"] * 64) >= 2, info
+    batch.run()
+    torch.cuda.synchronize()
+    _per_call_equal(reqs, interp)
+    batch.close()
+
+
+def test_resident_pairs_long_claims_match_per_call():
+    import torch
+    from noa_b200.batch import extract_batch_launch, volume_pairs
+    # pair-copy items are 64 x 16 pixels: more slices for the same number of claims
+    reqs, vols = _large_requests([(n, 4 * c) for n, c in LARGE], seed=5)
+    pairs = {n: volume_pairs(v, (1, n, n, n)) for n, v in vols.items()}
+    extract_batch_launch("hc2h", reqs, [pairs[r.slice_shape[2]] for r in reqs])
+    torch.cuda.synchronize()
+    _per_call_equal(reqs, "linear")
