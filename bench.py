@@ -309,7 +309,7 @@ def run_gpu(args) -> None:
             "gpu_launches": 4 * args.steps,
             "clocks": clocks.summary(),
         }
-        if not args.no_cpu_baseline:
+        if not args.no_cpu_baseline and world == 1:   # the CPU baseline is taken at N = 1 only
             line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
         print(json.dumps(line), flush=True)
     if world > 1:
