@@ -204,18 +204,31 @@ template<> struct AccElem<true, false> { using T = float2; };
 template<> struct AccElem<false, true> { using T = float2; };
 template<> struct AccElem<false, false> { using T = float; };
 
+// The reductions carry an L2 evict_last hint on half of the lines they touch: the accumulator is
+// slightly larger than the L2 and the slices stream past it, so keeping part of it resident saves
+// misses (2-3 % at 256^3 x 4096; a fraction of 1.0 gave 2 %).
+__device__ __forceinline__ unsigned long long acc_policy() {
+    unsigned long long pol;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 0.5;" : "=l"(pol));
+    return pol;
+}
+
 template<bool OUT_C, bool W>
 __device__ __forceinline__ void acc_add(void* acc, int off, float2 v, float w) {
     using T = typename AccElem<OUT_C, W>::T;
     T* p = static_cast<T*>(acc) + off;
+    const unsigned long long pol = acc_policy();
     if constexpr (OUT_C && W)
-        atomicAdd(p, make_float4(v.x, v.y, w, 0.f));
+        asm volatile("red.global.add.L2::cache_hint.v4.f32 [%0], {%1, %2, %3, %4}, %5;"
+                     :: "l"(p), "f"(v.x), "f"(v.y), "f"(w), "f"(0.f), "l"(pol) : "memory");
     else if constexpr (OUT_C)
-        atomicAdd(p, v);
+        asm volatile("red.global.add.L2::cache_hint.v2.f32 [%0], {%1, %2}, %3;"
+                     :: "l"(p), "f"(v.x), "f"(v.y), "l"(pol) : "memory");
     else if constexpr (W)
-        atomicAdd(p, make_float2(v.x, w));
+        asm volatile("red.global.add.L2::cache_hint.v2.f32 [%0], {%1, %2}, %3;"
+                     :: "l"(p), "f"(v.x), "f"(w), "l"(pol) : "memory");
     else
-        atomicAdd(p, v.x);
+        asm volatile("red.global.add.L2::cache_hint.f32 [%0], %1, %2;" :: "l"(p), "f"(v.x), "l"(pol) : "memory");
 }
 
 // Corner c = 4 c0 + 2 c1 + c2 of a cell; its offset from corner 0.
