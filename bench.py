@@ -7,7 +7,10 @@ Synthetic, seeded inputs: volume amplitude 1/max(|f|,1/64), slices complex Gauss
 uniform SO(3) orientations. Metric: slices/s (extract + insert slices per second, whole job).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-    python bench.py --workload insert_512     # 512^3 x 20,000 windowed-sinc insertion, gather vs scatter
+    python bench.py --workload insert_512          # 512^3 x 20,000 windowed-sinc insertion, gather vs scatter
+    python bench.py --workload insert_extract_256  # insert_and_extract, 4096 input -> 256 output slices
+    python bench.py --workload batched             # 12,000 LANCZOS8 extractions, 12 volumes, one launch
+Each workload line carries noa's CPU path timed on this host beside it (cpu_baseline).
 
 N > 1 runs under torchrun, one rank per GPU: every rank processes its own 4096 + 4096 slices (weak
 scaling; extraction needs no exchange, and the insertion's partial grids are summed by one NCCL
