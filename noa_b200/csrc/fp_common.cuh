@@ -466,6 +466,19 @@ struct View3 {
     Idx s0, s1, s2;
 };
 
+// Read-only 16-byte load whose line is kept in L2 with evict_last priority for half of the lines.
+// Volumes (and their pair copies) are about the size of the L2 or larger while the output slices
+// stream past them; keeping part of them resident saves re-reads (bit-identical; 1 % per extraction
+// call, 7 % for batched launches over pair copies).
+__device__ __forceinline__ float4 ldg_evict_last_half(const float4* p) {
+    unsigned long long pol;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 0.5;" : "=l"(pol));
+    float4 v;
+    asm volatile("ld.global.nc.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(p), "l"(pol));
+    return v;
+}
+
 template<bool CPLX, typename Idx>
 __device__ __forceinline__ float2 view_read(const View3<Idx>& v, Idx off) {
     if constexpr (CPLX)
@@ -588,7 +601,7 @@ __device__ __forceinline__ float2 interp_3d(const View3<Idx>& v, const Spectrum3
                                 float4 q[SIZE / 2];
 #pragma unroll
                                 for (int j = 0; j < SIZE / 2; ++j)
-                                    q[j] = __ldg(reinterpret_cast<const float4*>(e) + j);
+                                    q[j] = ldg_evict_last_half(reinterpret_cast<const float4*>(e) + j);
                                 const float2 last = odd ? __ldg(e + SIZE) : make_float2(0.f, 0.f);
 #pragma unroll
                                 for (int x = 0; x < SIZE; ++x) {

@@ -10,18 +10,6 @@
 
 namespace nb {
 
-// Read-only 16-byte load whose line is kept in L2 with evict_last priority for half of the lines: the
-// pair copy (16 bytes per voxel) is about the size of the L2 while the output slices stream past it,
-// so keeping part of it resident saves re-reads (1 % per call at 256^3, 7 % for batched launches).
-__device__ __forceinline__ float4 ldg_evict_last_half(const float4* p) {
-    unsigned long long pol;
-    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 0.5;" : "=l"(pol));
-    float4 v;
-    asm volatile("ld.global.nc.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
-                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(p), "l"(pol));
-    return v;
-}
-
 __device__ __forceinline__ float2 interp_linear_pairs(const float4* __restrict__ pairs, int sz, int sy,
                                                       const Spectrum3& sp, float q0, float q1, float q2) {
     float conjugate = 1.f;
