@@ -472,9 +472,9 @@ struct View3 {
 // call, 7 % for batched launches over pair copies).
 __device__ __forceinline__ float4 ldg_evict_last_half(const float4* p) {
     unsigned long long pol;
-    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 0.5;" : "=l"(pol));
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 0.5;" : "=l"(pol));
     float4 v;
-    asm volatile("ld.global.nc.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+    asm("ld.global.nc.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
                  : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(p), "l"(pol));
     return v;
 }

@@ -209,7 +209,7 @@ template<> struct AccElem<false, false> { using T = float; };
 // misses (2-3 % at 256^3 x 4096; a fraction of 1.0 gave 2 %).
 __device__ __forceinline__ unsigned long long acc_policy() {
     unsigned long long pol;
-    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 0.5;" : "=l"(pol));
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 0.5;" : "=l"(pol));
     return pol;
 }
 
