@@ -48,7 +48,11 @@ enum { NB_BATCH_AUTOTUNE = 1 };
 /* Validates the requests, uploads their descriptors, chooses the launch configuration (with
  * NB_BATCH_AUTOTUNE: by timing the candidates on this batch, once per workload key, cached in memory and
  * in the text file $NB_AUTOTUNE_CACHE or $HOME/.cache/noa_b200/autotune.txt; autotuning runs the batch,
- * so it writes the outputs) and captures the launch into a CUDA graph. Synchronizes `stream`. */
+ * so it writes the outputs) and captures the launch into a CUDA graph. Synchronizes `stream`.
+ * LINEAR batches over complex volumes (no scaling, EWS, input weights or w-window) hold a pair copy
+ * (16 bytes per rfft voxel) of each volume whose requests read at least twice as many pixels as it
+ * has voxels, like the per-call entry point; the graph rebuilds these copies at every run, so changes
+ * to the volumes between runs are seen. */
 NB_API int nb_extract_batch_create(int32_t remap, const nb_extract_request* requests, int64_t n_requests,
                                    const nb_options* options, int32_t flags, void* stream,
                                    nb_extract_batch* batch);

@@ -14,8 +14,9 @@
 //
 // nb_extract_batch_create validates every request like the per-call entry point, uploads the request
 // descriptors once, optionally autotunes (tile shape x CTAs per SM, timed on the batch itself and
-// cached per workload key in memory and in a small text file), and captures the launch — counter
-// reset + persistent kernel — into a CUDA graph. nb_extract_batch_run replays that graph on a stream.
+// cached per workload key in memory and in a small text file), and captures the launch — the pair
+// copies of LINEAR batches, counter reset, persistent kernel — into a CUDA graph.
+// nb_extract_batch_run replays that graph on a stream.
 #include "fp_args.cuh"
 #include "fp_pairs.cuh"
 #include "fp_pool.cuh"
@@ -24,8 +25,10 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <fstream>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <set>
 #include <sstream>
@@ -234,6 +237,79 @@ batch_extract_kernel(const BatchReq* __restrict__ reqs, int n_req, int64_t n_ite
     }
 }
 
+// Pairs-only batches of at most PACK requests pass their descriptors as a kernel parameter: the
+// request fields are then read through the constant bank like a per-call kernel's arguments, with no
+// staging in shared memory and no barrier when a CTA's request changes (28.4 KB of parameters, within
+// the 32 KB that sm_70+ kernels accept).
+constexpr int PACK = 48;
+struct ReqPack { BatchReq r[PACK]; };
+static_assert(sizeof(ReqPack) + 64 <= 32764, "the descriptor pack must fit the kernel parameter space");
+
+template<bool OUT_C>
+__global__ void __launch_bounds__(256, 6)
+batch_pairs_param_kernel(const __grid_constant__ ReqPack pack, int n_req, int64_t n_items,
+                         unsigned long long* __restrict__ counter) {
+    constexpr Variant VT = VARIANTS[0];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    constexpr int WARPS_X = VT.tx / VT.wx;
+    const int ly = (warp / WARPS_X) * VT.wy + lane / VT.wx;
+    const int lx = (warp % WARPS_X) * VT.wx + lane % VT.wx;
+    int found = 0;
+    const long long per_cta = n_items / (static_cast<long long>(gridDim.x) * 64);
+    const long long chunk = per_cta < 1 ? 1 : (per_cta > 64 ? 64 : per_cta);
+    __shared__ long long s_chunk[2];
+    long long next = threadIdx.x == 0 ? static_cast<long long>(atomicAdd(counter, static_cast<unsigned long long>(chunk))) : 0;
+    for (int round = 0;; ++round) {
+        if (threadIdx.x == 0) {
+            s_chunk[round & 1] = next;
+            if (next < n_items)
+                next = static_cast<long long>(atomicAdd(counter, static_cast<unsigned long long>(chunk)));
+        }
+        __syncthreads();
+        const long long c0 = s_chunk[round & 1];
+        if (c0 >= n_items)
+            break;
+        const long long c1 = c0 + chunk < n_items ? c0 + chunk : n_items;
+        int64_t b = 0;
+        int ty = 0, tx = 0, nty = 1;
+        bool fresh = true;
+        for (long long item = c0; item < c1; ++item) {
+            if (found + 1 < n_req && pack.r[found + 1].first_item <= item) {
+                int lo = found + 1, hi = n_req - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) / 2;
+                    if (pack.r[mid].first_item <= item)
+                        lo = mid;
+                    else
+                        hi = mid - 1;
+                }
+                found = lo;
+                fresh = true;
+            }
+            const BatchReq& R = pack.r[found];
+            if (fresh) {
+                const int64_t local = item - R.first_item;
+                b = local / R.tiles_per_slice;
+                const int tile = static_cast<int>(local - b * R.tiles_per_slice);
+                ty = tile / R.ntx;
+                tx = tile - ty * R.ntx;
+                nty = R.tiles_per_slice / R.ntx;
+                fresh = false;
+            }
+            const int u = tx * VT.tx + lx;
+            if (u < R.a.slice_w / 2 + 1)
+                extract_rows_pairs<OUT_C>(R.a, R.pairs, b, ty * (VT.ty * PAIRS_PPT) + ly, VT.ty, u);
+            if (++tx == R.ntx) {
+                tx = 0;
+                if (++ty == nty) {
+                    ty = 0;
+                    ++b;
+                }
+            }
+        }
+    }
+}
+
 using KernelFn = void (*)(const BatchReq*, int, int64_t, unsigned long long*);
 
 template<int I, bool IN_C, bool OUT_C>
@@ -345,6 +421,10 @@ struct nb_extract_batch_t {
     std::string key;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    // LINEAR batches: pair copies of the volumes read enough to amortise one, rebuilt by every run
+    // (their make_pairs launches are part of the graph), so later changes to the volumes are seen.
+    std::vector<std::pair<nb::ProjArgs, float4*>> pair_jobs;
+    bool pairs_only = false;  // every request reads a pair copy: the pairs-only kernel
 };
 
 namespace nb {
@@ -384,12 +464,53 @@ cudaError_t upload(nb_extract_batch_t* h, int variant, cudaStream_t stream) {
     return cudaStreamSynchronize(stream);
 }
 
+KernelFn pairs_only_kernel(bool out_c) {
+    return out_c ? batch_extract_kernel<I_LINEAR, true, true, 0, true> : batch_extract_kernel<I_LINEAR, true, false, 0, true>;
+}
+
+int param_blocks_per_sm(bool out_c) {
+    int n = 0;
+    const cudaError_t e = out_c ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_pairs_param_kernel<true>, 256, 0)
+                                : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_pairs_param_kernel<false>, 256, 0);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    return n > 0 ? n : 1;
+}
+
+// The pairs-only kernel with the descriptors (tile fields set for variant 0) as its parameter.
+cudaError_t launch_param(const std::vector<BatchReq>& reqs, int64_t n_items, bool out_c, int blocks_per_sm,
+                         unsigned long long* counter, cudaStream_t s) {
+    auto pack = std::make_unique<ReqPack>();
+    std::memset(static_cast<void*>(pack.get()), 0, sizeof(ReqPack));
+    std::copy(reqs.begin(), reqs.end(), pack->r);
+    const int n = static_cast<int>(reqs.size());
+    const int grid = sm_count() * blocks_per_sm;
+    if (out_c)
+        batch_pairs_param_kernel<true><<<grid, 256, 0, s>>>(*pack, n, n_items, counter);
+    else
+        batch_pairs_param_kernel<false><<<grid, 256, 0, s>>>(*pack, n, n_items, counter);
+    return cudaGetLastError();
+}
+
+bool use_param(const nb_extract_batch_t* h) {
+    return h->pairs_only && h->host_reqs.size() <= static_cast<size_t>(PACK);
+}
+
 cudaError_t launch(nb_extract_batch_t* h, const Config& c, cudaStream_t stream) {
-    const KernelFn fn = pick_kernel(h->interp, h->in_cplx, h->out_cplx, c.variant);
+    const KernelFn fn = h->pairs_only ? pairs_only_kernel(h->out_cplx)
+                                      : pick_kernel(h->interp, h->in_cplx, h->out_cplx, c.variant);
     const int grid = sm_count() * c.blocks_per_sm;
-    cudaError_t err = cudaMemsetAsync(h->d_counter, 0, sizeof(unsigned long long), stream);
+    cudaError_t err = cudaSuccess;
+    for (const auto& job : h->pair_jobs)
+        if ((err = launch_make_pairs(job.first, job.second, stream)) != cudaSuccess)
+            return err;
+    err = cudaMemsetAsync(h->d_counter, 0, sizeof(unsigned long long), stream);
     if (err != cudaSuccess)
         return err;
+    if (use_param(h))
+        return launch_param(h->host_reqs, h->n_items, h->out_cplx, c.blocks_per_sm, h->d_counter, stream);
     fn<<<grid, 256, 0, stream>>>(h->d_reqs, static_cast<int>(h->host_reqs.size()), h->n_items, h->d_counter);
     return cudaGetLastError();
 }
@@ -424,6 +545,50 @@ double time_config(nb_extract_batch_t* h, const Config& c, cudaStream_t stream, 
     return result;
 }
 
+// LINEAR over complex volumes: a pair copy per distinct volume whose requests read at least twice
+// as many pixels as it has voxels (the per-call rule), allocated for the batch's lifetime. Without
+// memory for a copy, its requests take the generic path.
+void plan_pairs(nb_extract_batch_t* h) {
+    if (h->interp != I_LINEAR || !h->in_cplx)
+        return;
+    struct Vol { const ProjArgs* a; int64_t pixels; std::vector<size_t> reqs; };
+    std::vector<Vol> vols;
+    for (size_t i = 0; i < h->host_reqs.size(); ++i) {
+        const ProjArgs& a = h->host_reqs[i].a;
+        if (!pairs_apply(a))
+            continue;
+        Vol* v = nullptr;
+        for (Vol& c : vols)
+            if (c.a->in.data == a.in.data && c.a->vol_d == a.vol_d && c.a->vol_h == a.vol_h &&
+                c.a->vol_w == a.vol_w && c.a->in.s0 == a.in.s0 && c.a->in.s1 == a.in.s1 &&
+                c.a->in.s2 == a.in.s2 && c.a->in_centered == a.in_centered)
+                v = &c;
+        if (!v) {
+            vols.push_back({&a, 0, {}});
+            v = &vols.back();
+        }
+        v->pixels += a.n_slices * a.slice_h * static_cast<int64_t>(a.slice_w / 2 + 1);
+        v->reqs.push_back(i);
+    }
+    for (const Vol& v : vols) {
+        const int64_t vox = static_cast<int64_t>(v.a->vol_d) * v.a->vol_h * (v.a->vol_w / 2 + 1);
+        if (v.pixels < 2 * vox)
+            continue;
+        float4* buf = nullptr;
+        if (cudaMalloc(&buf, static_cast<size_t>(vox) * sizeof(float4)) != cudaSuccess) {
+            cudaGetLastError();
+            continue;
+        }
+        h->pair_jobs.push_back({*v.a, buf});
+        for (size_t i : v.reqs)
+            h->host_reqs[i].pairs = buf;
+    }
+    bool all = !h->host_reqs.empty();
+    for (const BatchReq& r : h->host_reqs)
+        all = all && r.pairs != nullptr;
+    h->pairs_only = all;
+}
+
 std::string workload_key(const nb_extract_batch_t* h) {
     std::set<std::string> boxes;
     int64_t slices = 0;
@@ -449,6 +614,8 @@ void release(nb_extract_batch_t* h) {
     if (h->graph) cudaGraphDestroy(h->graph);
     if (h->d_reqs) cudaFree(h->d_reqs);
     if (h->d_counter) cudaFree(h->d_counter);
+    for (auto& job : h->pair_jobs)
+        cudaFree(job.second);
     delete h;
 }
 
@@ -460,6 +627,18 @@ int launch_once(nb_extract_batch_t& h, KernelFn fn, int variant, int blocks_per_
         set_tiles(r, vt, first);
     if (first == 0)
         return finish_launch(cudaSuccess);
+    if (fn == nullptr) {
+        // Pairs-only with the descriptors as the kernel parameter: only the counter is allocated.
+        void* dev = scratch_alloc(sizeof(unsigned long long), s);
+        if (!dev)
+            return report_error(NB_ERROR_OOM, "cannot allocate the batch work counter");
+        auto* d_counter = static_cast<unsigned long long*>(dev);
+        cudaError_t err = cudaMemsetAsync(d_counter, 0, sizeof(unsigned long long), s);
+        if (err == cudaSuccess)
+            err = launch_param(h.host_reqs, first, h.out_cplx, blocks_per_sm, d_counter, s);
+        scratch_free(dev, s);
+        return finish_launch(err);
+    }
     // Descriptors then the work counter, in one stream-ordered allocation.
     const size_t desc_bytes = (h.host_reqs.size() * sizeof(BatchReq) + 255) / 256 * 256;
     void* dev = scratch_alloc(desc_bytes + sizeof(unsigned long long), s);
@@ -522,6 +701,7 @@ int nb_extract_batch_create(int32_t remap, const nb_extract_request* requests, i
         h->host_reqs[static_cast<size_t>(i)].a = a;
         h->host_reqs[static_cast<size_t>(i)].pairs = nullptr;
     }
+    plan_pairs(h);
     if (cudaMalloc(&h->d_reqs, h->host_reqs.size() * sizeof(BatchReq)) != cudaSuccess ||
         cudaMalloc(&h->d_counter, sizeof(unsigned long long)) != cudaSuccess) {
         cudaGetLastError();
@@ -529,11 +709,14 @@ int nb_extract_batch_create(int32_t remap, const nb_extract_request* requests, i
         return report_error(NB_ERROR_OOM, "cannot allocate the batch descriptors");
     }
 
-    // Configuration: autotuned (cached per workload key), or the default.
+    // Configuration: autotuned (cached per workload key), or the default. With a pair copy for every
+    // request, the pairs-only kernel at full occupancy (as the one-shot launch uses).
     h->key = workload_key(h);
-    Config best{0, max_blocks_per_sm(pick_kernel(h->interp, h->in_cplx, h->out_cplx, 0))};
-    bool tuned = false;
-    if (flags & NB_BATCH_AUTOTUNE) {
+    Config best{0, use_param(h) ? param_blocks_per_sm(h->out_cplx)
+                                : max_blocks_per_sm(h->pairs_only ? pairs_only_kernel(h->out_cplx)
+                                                                  : pick_kernel(h->interp, h->in_cplx, h->out_cplx, 0))};
+    bool tuned = h->pairs_only;
+    if ((flags & NB_BATCH_AUTOTUNE) && !tuned) {
         std::lock_guard<std::mutex> lock(g_tune_mutex);
         load_cache_locked();
         auto it = g_tuned.find(h->key);
@@ -661,9 +844,11 @@ int nb_extract_batch_launch(int32_t remap, const nb_extract_request_ex* requests
     h.key = workload_key(&h);
     Config cfg{0, 0};
     if (all_pairs) {
-        // Pair copies everywhere: the lean pairs-only kernel, tile 64 x 16, full occupancy.
-        const KernelFn fn = h.out_cplx ? batch_extract_kernel<I_LINEAR, true, true, 0, true>
-                                       : batch_extract_kernel<I_LINEAR, true, false, 0, true>;
+        // Pair copies everywhere: the lean pairs-only kernel, tile 64 x 16, full occupancy; with few
+        // requests, their descriptors travel as its parameter.
+        if (h.host_reqs.size() <= static_cast<size_t>(PACK))
+            return launch_once(h, nullptr, 0, param_blocks_per_sm(h.out_cplx), s);
+        const KernelFn fn = pairs_only_kernel(h.out_cplx);
         return launch_once(h, fn, 0, max_blocks_per_sm(fn), s);
     }
     {

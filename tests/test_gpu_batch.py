@@ -117,7 +117,8 @@ def test_batch_long_claims_match_per_call(interp, tmp_path, monkeypatch):
     import torch
     from noa_b200.batch import ExtractBatch
     monkeypatch.setenv("NB_AUTOTUNE_CACHE", str(tmp_path / "autotune.txt"))
-    reqs, _ = _large_requests(LARGE)
+    # LINEAR batches read pair copies, whose items are 64 x 16 pixels: 4x the slices for as many claims
+    reqs, _ = _large_requests([(n, 4 * c) for n, c in LARGE] if interp == "linear" else LARGE)
     batch = ExtractBatch("hc2h", reqs, interp=interp, autotune=False)
     info = batch.info()
     assert info["n_items"] // (info["grid"] * 64) >= 2, info
@@ -136,3 +137,24 @@ def test_resident_pairs_long_claims_match_per_call():
     extract_batch_launch("hc2h", reqs, [pairs[r.slice_shape[2]] for r in reqs])
     torch.cuda.synchronize()
     _per_call_equal(reqs, "linear")
+
+
+def test_linear_batch_pair_copies_follow_volume_updates(tmp_path, monkeypatch):
+    """LINEAR batches read pair copies that the graph rebuilds at every run: a volume changed between
+    runs is seen, and results stay those of the per-call entry point."""
+    import torch
+    from noa_b200.batch import ExtractBatch
+    monkeypatch.setenv("NB_AUTOTUNE_CACHE", str(tmp_path / "autotune.txt"))
+    reqs, vols = _large_requests([(64, 300), (96, 150), (64, 40)], seed=9)
+    batch = ExtractBatch("hc2h", reqs, interp="linear", autotune=True)
+    batch.run()
+    torch.cuda.synchronize()
+    _per_call_equal(reqs, "linear")
+    for v in vols.values():
+        v.mul_(-0.5).add_(0.25)
+    for r in reqs:
+        r.slice.fill_(3)
+    batch.run()
+    torch.cuda.synchronize()
+    _per_call_equal(reqs, "linear")
+    batch.close()
