@@ -304,7 +304,10 @@ def run_gpu(args) -> None:
                        "rasterize_gbs": ab["rasterize"] / (ras_ms * 1e-3) / 1e9},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peaks["hbm_gbs"],
                          "peak_source": peaks["source"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
-                         "algorithmic_bytes": ab[dom], "traffic": traffic.get(dom)},
+                         "algorithmic_bytes": ab[dom], "traffic": traffic.get(dom),
+                         # what ncu shows bounds the kernel on chip (HBM is not the limit of either)
+                         "limiter": {"rasterize": "L2 tag requests of the scatter's reductions",
+                                     "extract": "L1 data pipe of the tap gathers"}[dom]},
             "e2e": {"value": total_slices / (e2e * 1e-3), "unit": "slices/s", "h2d_bytes_per_step": bi,
                     "d2h_bytes_per_step": bo, "ms_per_step": e2e,
                     "schedule": f"{E2E_CHUNKS} slice chunks; copies in, kernels and copies out on 3 streams"},
