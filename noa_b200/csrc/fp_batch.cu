@@ -627,18 +627,6 @@ int launch_once(nb_extract_batch_t& h, KernelFn fn, int variant, int blocks_per_
         set_tiles(r, vt, first);
     if (first == 0)
         return finish_launch(cudaSuccess);
-    if (fn == nullptr) {
-        // Pairs-only with the descriptors as the kernel parameter: only the counter is allocated.
-        void* dev = scratch_alloc(sizeof(unsigned long long), s);
-        if (!dev)
-            return report_error(NB_ERROR_OOM, "cannot allocate the batch work counter");
-        auto* d_counter = static_cast<unsigned long long*>(dev);
-        cudaError_t err = cudaMemsetAsync(d_counter, 0, sizeof(unsigned long long), s);
-        if (err == cudaSuccess)
-            err = launch_param(h.host_reqs, first, h.out_cplx, blocks_per_sm, d_counter, s);
-        scratch_free(dev, s);
-        return finish_launch(err);
-    }
     // Descriptors then the work counter, in one stream-ordered allocation.
     const size_t desc_bytes = (h.host_reqs.size() * sizeof(BatchReq) + 255) / 256 * 256;
     void* dev = scratch_alloc(desc_bytes + sizeof(unsigned long long), s);
@@ -844,10 +832,9 @@ int nb_extract_batch_launch(int32_t remap, const nb_extract_request_ex* requests
     h.key = workload_key(&h);
     Config cfg{0, 0};
     if (all_pairs) {
-        // Pair copies everywhere: the lean pairs-only kernel, tile 64 x 16, full occupancy; with few
-        // requests, their descriptors travel as its parameter.
-        if (h.host_reqs.size() <= static_cast<size_t>(PACK))
-            return launch_once(h, nullptr, 0, param_blocks_per_sm(h.out_cplx), s);
+        // Pair copies everywhere: the lean pairs-only kernel, tile 64 x 16, full occupancy. (The
+        // parameter-descriptor kernel is for captured graphs only: launched one-shot from a serving
+        // loop, its 28 KB of parameters per launch made the loop's tail latency 5x worse.)
         const KernelFn fn = pairs_only_kernel(h.out_cplx);
         return launch_once(h, fn, 0, max_blocks_per_sm(fn), s);
     }
