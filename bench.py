@@ -10,6 +10,7 @@ uniform SO(3) orientations. Metric: slices/s (extract + insert slices per second
     python bench.py --workload insert_512          # 512^3 x 20,000 windowed-sinc insertion, gather vs scatter
     python bench.py --workload insert_extract_256  # insert_and_extract, 4096 input -> 256 output slices
     python bench.py --workload batched             # 12,000 LANCZOS8 extractions, 12 volumes, one launch
+    python bench.py --workload extract_wwindow_256 # 4096 extractions with a 7-sample w-windowed sinc
 Each workload line carries noa's CPU path timed on this host beside it (cpu_baseline).
 
 N > 1 runs under torchrun, one rank per GPU: every rank processes its own 4096 + 4096 slices (weak
@@ -648,6 +649,87 @@ def _insert_extract_cpu_baseline(h_in, h_rot_in, h_rot_out, n: int, total: int) 
 
 
 # ---------------------------------------------------------------------------------------------------
+# w-windowed-sinc extraction (noa's 4-D FourierExtract): every pixel sums the windowed samples of a
+# short z window of the volume.
+# ---------------------------------------------------------------------------------------------------
+WW_SINC, WW_BLACKMAN = 2.0, 4.0   # in voxels of the z axis: fftfreq 2/256 and 4/256 (a 7-sample window)
+
+
+def run_extract_wwindow(args) -> None:
+    """extract_central_slices_3d<"hc2h"> of 4096 slices of 256x129 c64 from a 256^3 volume, LINEAR, with
+    the w-windowed sinc {fftfreq_sinc 2/256, fftfreq_blackman 4/256} (7 z samples per pixel), cutoff 0.5.
+    noa's CPU path runs the first slices of the same job beside it, and they are compared."""
+    import torch
+    from noa_b200 import fourier_project as fp
+    from noa_b200 import synthetic
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    n, nsl = args.n, args.slices
+    wp = n // 2 + 1
+    h_vol = synthetic.make_volume(n, seed=31)
+    vol = torch.from_numpy(h_vol).to(dev)
+    rot_h = synthetic.random_rotations(nsl, seed=32)
+    rot = fp.pack_rotations(torch.from_numpy(rot_h).to(dev))
+    out = torch.empty((nsl, 1, n, wp), dtype=torch.complex64, device=dev)
+    wws = fp.WindowedSinc(WW_SINC / n, WW_BLACKMAN / n)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+
+    def call():
+        fp.extract_central_slices_3d("hc2h", vol, None, (1, n, n, n), out, None, (nsl, 1, n, n), None, rot,
+                                     interp="linear", w_windowed_sinc=wws)
+
+    for _ in range(max(args.warmup, 3)):
+        call()
+    torch.cuda.synchronize()
+    ts = []
+    with ClockSampler(0) as clocks:
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            call()
+            b.record()
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b))
+    ms = statistics.median(ts)
+    alg = 8 * n * n * wp + nsl * (8 * n * wp + 48)
+    peaks = measured_peaks()
+    achieved = alg / (ms * 1e-3) / 1e9
+    line = {
+        "metric": f"slices/sec w-windowed extraction at {n}^3", "value": nsl / (ms * 1e-3), "unit": "slices/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded; no dataset)",
+        "config": {"workload": f"extract {nsl} slices of {n}x{wp} c64 from a {n}^3 rfft volume, hc2h, LINEAR, "
+                               f"w-windowed sinc {{{WW_SINC:g}/{n}, {WW_BLACKMAN:g}/{n}}} (7 z samples per pixel)",
+                   "l2": "flushed between steps"},
+        "roofline": {"bound": "hbm", "kernel": "extract_kernel", "achieved": achieved, "peak": peaks["hbm_gbs"],
+                     "peak_source": peaks["source"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+                     "algorithmic_bytes": alg, "traffic": None},
+        "gpu_launches": args.steps,
+        "clocks": clocks.summary(),
+    }
+    if not args.no_cpu_baseline:
+        from oracle.oracle import Call
+        kind, run = _cpu_impl()
+        threads = os.cpu_count() or 1
+        # noa iterates (slice, w, y, x) and gives a thread at least 2^20 of them
+        k = min(nsl, max(8, -(-threads * NOA_INDICES_PER_THREAD // (7 * n * wp))))
+        c = Call(func="extract", remap="hc2h", inp=h_vol, in_shape=(1, n, n, n),
+                 out=np.zeros((k, 1, n, wp), np.complex64), out_shape=(k, 1, n, n), rot=rot_h[:k],
+                 interp=1, cutoff=0.5, w_sinc=(WW_SINC / n, WW_BLACKMAN / n))
+        t0 = time.perf_counter()
+        run(c, threads)
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": k / dt, "unit": "slices/s", "cores": threads, "kind": kind,
+                                "sample": f"the first {k} of the {nsl} slices in {dt:.1f} s, threads={threads}"}
+        o = out[:k].cpu().numpy().astype(np.complex128)
+        ref = c.out.astype(np.complex128)
+        line["cpu_sample_rel_l2"] = float(np.linalg.norm(o - ref) / np.linalg.norm(ref))
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------------------------------
 # Fourth workload: batched uneven LANCZOS8 extraction (persistent kernel in a CUDA graph).
 # ---------------------------------------------------------------------------------------------------
 def run_batched(args) -> None:
@@ -724,16 +806,24 @@ def main() -> None:
                    help="slices per CPU call of the reference arm (default: enough for noa to use every thread)")
     p.add_argument("--n", type=int, default=None, help="box size (default 256, or 512 for insert_512)")
     p.add_argument("--slices", type=int, default=None, help="slices per op per step")
-    p.add_argument("--workload", choices=["extract_insert_256", "insert_512", "insert_extract_256", "batched"],
+    p.add_argument("--workload", choices=["extract_insert_256", "insert_512", "insert_extract_256", "batched",
+                                          "extract_wwindow_256"],
                    default="extract_insert_256",
                    help="insert_512: the 512^3 x 20,000 windowed-sinc insertion, gather vs scatter form; "
                         "insert_extract_256: insert_and_extract_central_slices_3d, 4096 in, 256 out; "
-                        "batched: 12,000 LANCZOS8 extractions over 12 volumes in one persistent launch")
+                        "batched: 12,000 LANCZOS8 extractions over 12 volumes in one persistent launch; "
+                        "extract_wwindow_256: 4096 extractions with a 7-sample w-windowed sinc")
     p.add_argument("--out-slices", type=int, default=256, help="insert_extract_256: output slices")
     p.add_argument("--ref-slices", type=int, default=None,
                    help="slices of the CPU reference sample (insert_512: 64 input, insert_extract_256: 2 output)")
     args = p.parse_args()
     global N, SLICES
+    if args.workload == "extract_wwindow_256":
+        args.n = args.n or 256
+        args.slices = args.slices or 4096
+        args.steps = min(args.steps, 20)
+        run_extract_wwindow(args)
+        return
     if args.workload == "batched":
         args.slices = args.slices or 12000
         args.steps = min(args.steps, 5)

@@ -87,12 +87,62 @@ extract_pairs_kernel(const __grid_constant__ ProjArgs a, const float4* __restric
     }
 }
 
+// The w-windowed form over the pair copy: per pixel, the windowed sum over the w offsets of the
+// z-shifted samples, each read as 4 pair loads — extract_kernel's w loop step for step (same offsets,
+// cutoff tests, window values and sum order), so the results are bit-identical to it.
+template<bool OUT_C>
+__global__ void __launch_bounds__(EXTRACT_THREADS)
+extract_pairs_w_kernel(const __grid_constant__ ProjArgs a, const float4* __restrict__ pairs, int ntx) {
+    const int wp = a.slice_w / 2 + 1;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int y0 = (blockIdx.x / ntx) * (TY * PAIR_PPT) + (warp >> 1) * 4 + (lane >> 3);
+    const int u = (blockIdx.x % ntx) * TX + (warp & 1) * 8 + (lane & 7);
+    if (u >= wp)
+        return;
+    const Spectrum3 sp{a.vol_d, a.vol_h, a.vol_w, a.in_centered};
+    const int WP = a.vol_w / 2 + 1;
+    const int sz = a.vol_h * WP, sy = WP;
+    const bool has_out_w = a.out_w.present;
+    const float f1 = div(static_cast<float>(u), a.f_slice1);
+
+    for (int64_t b = blockIdx.y; b < a.n_slices; b += gridDim.y) {
+#pragma unroll 1
+        for (int r = 0; r < PAIR_PPT; ++r) {
+            const int y = y0 + r * TY;
+            if (y >= a.slice_h)
+                break;
+            const float f0 = div(static_cast<float>(index2frequency(a.out_centered, y, a.slice_h)), a.f_slice0);
+            float fz, fy, fx;
+            slice2grid(f0, f1, a.scale, a.rot, b, a.ews, fz, fy, fx);
+            float2 value = make_float2(0.f, 0.f);
+            float weight = 0.f;
+            for (int w = 0; w < a.wsize; ++w) {
+                const float off = div(static_cast<float>(w - a.wsize / 2), a.target0);
+                const float gz = add(fz, off);
+                if (dot3(gz, fy, fx, gz, fy, fx) > a.cutoff_sqd)
+                    continue;
+                const float cw = windowed_sinc(off, a.efs, a.efb);
+                const float2 iv = to_output<true, OUT_C>(interp_linear_pairs(
+                    pairs, sz, sy, sp, mul(gz, a.target0), mul(fy, a.target1), mul(fx, a.target2)));
+                value = cadd(value, cmul(iv, cw));
+                if (has_out_w)
+                    weight = add(weight, mul(1.f, cw));
+            }
+            dst_store_stream<OUT_C>(a.out, b, y, u, value);
+            if (has_out_w)
+                store_real_stream(a.out_w, b, y, u, weight);
+        }
+    }
+}
+
 // Whether the per-call pair path applies: the pair copy is readable (pairs_apply) and there are enough
 // pixels to amortise making it.
 bool use_pairs(const ProjArgs& a) {
     const int64_t vox = static_cast<int64_t>(a.vol_d) * a.vol_h * (a.vol_w / 2 + 1);
     const int64_t pix = a.n_slices * a.slice_h * static_cast<int64_t>(a.slice_w / 2 + 1);
-    return pairs_apply(a) && pix >= 2 * vox;
+    ProjArgs plain = a;
+    plain.wsize = 1;  // the w-windowed form reads the pair copy too (extract_pairs_w_kernel)
+    return pairs_apply(plain) && pix >= 2 * vox;
 }
 
 cudaError_t launch_pairs(const ProjArgs& a, cudaStream_t stream, bool& done) {
@@ -106,10 +156,16 @@ cudaError_t launch_pairs(const ProjArgs& a, cudaStream_t stream, bool& done) {
     const int wp = a.slice_w / 2 + 1;
     const int ntx = (wp + TX - 1) / TX, nty = (a.slice_h + TY * PAIR_PPT - 1) / (TY * PAIR_PPT);
     const dim3 grid(static_cast<unsigned>(ntx * nty), static_cast<unsigned>(a.n_slices < 65535 ? a.n_slices : 65535));
-    if (a.out_cplx)
+    if (a.wsize > 1) {
+        if (a.out_cplx)
+            extract_pairs_w_kernel<true><<<grid, EXTRACT_THREADS, 0, stream>>>(a, pairs, ntx);
+        else
+            extract_pairs_w_kernel<false><<<grid, EXTRACT_THREADS, 0, stream>>>(a, pairs, ntx);
+    } else if (a.out_cplx) {
         extract_pairs_kernel<true><<<grid, EXTRACT_THREADS, 0, stream>>>(a, pairs, ntx);
-    else
+    } else {
         extract_pairs_kernel<false><<<grid, EXTRACT_THREADS, 0, stream>>>(a, pairs, ntx);
+    }
     const cudaError_t err = cudaGetLastError();
     scratch_free(pairs, stream);
     done = err == cudaSuccess;

@@ -162,6 +162,32 @@ def test_gpu_extract_pair_path_bit_identical_to_generic():
     np.testing.assert_array_equal(a, b)
 
 
+@pytest.mark.parametrize("remap", ["h2h", "hc2hc"])
+@pytest.mark.parametrize("out_dt", ["c32", "f32"])
+def test_gpu_extract_pair_path_w_window(remap, out_dt):
+    """The w-windowed extraction through the pair copy (5-sample window, enough slices)."""
+    import gpu_run
+    call = build(default_case("extract", remap=remap, n=32, nslices=80, out_dt=out_dt, out_w=True,
+                              w_sinc=(1.5 / 32, 3.0 / 32), seed=642))
+    ref = clone(call)
+    FpOracle().run(ref, 8)
+    out, out_w = gpu_run.run(clone(call))
+    assert rel_l2(out, ref.out) <= 1e-5
+    assert rel_l2(out_w, ref.out_w) <= 1e-5
+
+
+def test_gpu_extract_pair_path_w_window_bit_identical_to_generic():
+    """With the w-window too, the pair path and the generic path give identical bits."""
+    import gpu_run
+    call = build(default_case("extract", remap="hc2h", n=48, nslices=96, out_w=True, w_sinc=(2.0 / 48, 4.0 / 48),
+                              seed=643))
+    a, aw = gpu_run.run(clone(call))
+    call.scale = np.repeat(np.eye(2, dtype=np.float32)[None], 96, axis=0)
+    b, bw = gpu_run.run(clone(call))
+    np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(aw, bw)
+
+
 @pytest.mark.parametrize("out_w", [False, True])
 @pytest.mark.parametrize("dts", [("c32", "c32"), ("c32", "f32"), ("f32", "f32")])
 def test_gpu_rasterize_accumulator_paths(out_w, dts):
