@@ -7,7 +7,7 @@
 // 32-bit whenever the volume fits, and the LINEAR path resolves bounds and frequency2index once per
 // axis rather than once per tap. LINEAR extraction of a complex volume with enough pixels first makes
 // a pair copy of the volume (fp_pairs.cuh) and reads each trilinear cell as four 16-byte loads, four
-// pixels per thread (extract_pairs_kernel).
+// pixels per thread (extract_pairs_kernel; extract_pairs_w_kernel with the w-window).
 //
 // The w-windowed form (wsize > 1) keeps the reference's semantics — outputs are the windowed sum over
 // the w offsets of the z-shifted samples — but sums in registers, in w order, instead of zeroing the
