@@ -55,11 +55,13 @@ __device__ __forceinline__ float2 interp_linear_pairs(const float4* __restrict__
 }
 
 // Whether a call may read the pair copy: LINEAR, complex volume given as an array, no input weights,
-// no EWS, no scaling, no w-window, a copy addressable in 32 bits.
+// no w-window (per-call extractions take extract_pairs_w_kernel for that), a copy addressable in 32
+// bits. Scaling and the Ewald-sphere curvature only change the coordinates (slice2grid), which the
+// pair kernels compute as the generic ones do.
 inline bool pairs_apply(const ProjArgs& a) {
     const int64_t vox = static_cast<int64_t>(a.vol_d) * a.vol_h * (a.vol_w / 2 + 1);
-    return a.interp == I_LINEAR && a.in_cplx && !a.in_w.present && !a.in.is_value && !a.ews.on &&
-           a.scale.kind == 0 && a.wsize <= 1 && vox < (int64_t(1) << 31);
+    return a.interp == I_LINEAR && a.in_cplx && !a.in_w.present && !a.in.is_value && a.wsize <= 1 &&
+           vox < (int64_t(1) << 31);
 }
 
 // Writes the pair copy of a.in (a.vol_d x a.vol_h x a.vol_w/2+1 complex values) to `pairs`.

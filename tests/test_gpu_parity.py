@@ -151,15 +151,37 @@ def test_gpu_extract_pair_path(remap, out_dt):
     assert rel_l2(out_w, ref.out_w) <= 1e-5
 
 
-def test_gpu_extract_pair_path_bit_identical_to_generic():
-    """The pair path and the generic path (forced by an identity scaling) give identical bits."""
-    import torch
+def _generic_forced(call):
+    """The same extraction through the generic kernel: input weights (which change only the output
+    weights) keep a call off the pair copy."""
+    c = clone(call)
+    c.inp_w = np.ones(call.inp.shape, np.float32)
+    return c
+
+
+@pytest.mark.parametrize("variant", ["plain", "scaled", "ews"])
+def test_gpu_extract_pair_path_bit_identical_to_generic(variant):
+    """The pair path and the generic path give identical values, also with scaling and the Ewald
+    curvature (which the pair kernels compute through the same slice2grid)."""
     import gpu_run
-    call = build(default_case("extract", remap="hc2h", n=48, nslices=96, seed=641))
+    kw = {"scaled": dict(scale=True), "ews": dict(ews=(45.0, 60.0))}.get(variant, {})
+    call = build(default_case("extract", remap="hc2h", n=48, nslices=96, seed=641, **kw))
     a, _ = gpu_run.run(clone(call))
-    call.scale = np.repeat(np.eye(2, dtype=np.float32)[None], 96, axis=0)
-    b, _ = gpu_run.run(clone(call))
+    b, _ = gpu_run.run(_generic_forced(call))
     np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("variant", ["scaled", "ews"])
+def test_gpu_extract_pair_path_scaled_or_curved(variant):
+    """Scaled and curved extractions through the pair copy, against the oracle."""
+    import gpu_run
+    kw = {"scaled": dict(scale=True), "ews": dict(ews=(45.0, 60.0))}[variant]
+    call = build(default_case("extract", remap="h2hc", n=32, nslices=80, out_w=True, seed=644, **kw))
+    ref = clone(call)
+    FpOracle().run(ref, 8)
+    out, out_w = gpu_run.run(clone(call))
+    assert rel_l2(out, ref.out) <= 1e-5
+    assert rel_l2(out_w, ref.out_w) <= 1e-5
 
 
 @pytest.mark.parametrize("remap", ["h2h", "hc2hc"])
@@ -181,11 +203,9 @@ def test_gpu_extract_pair_path_w_window_bit_identical_to_generic():
     import gpu_run
     call = build(default_case("extract", remap="hc2h", n=48, nslices=96, out_w=True, w_sinc=(2.0 / 48, 4.0 / 48),
                               seed=643))
-    a, aw = gpu_run.run(clone(call))
-    call.scale = np.repeat(np.eye(2, dtype=np.float32)[None], 96, axis=0)
-    b, bw = gpu_run.run(clone(call))
+    a, _ = gpu_run.run(clone(call))
+    b, _ = gpu_run.run(_generic_forced(call))
     np.testing.assert_array_equal(a, b)
-    np.testing.assert_array_equal(aw, bw)
 
 
 @pytest.mark.parametrize("out_w", [False, True])
