@@ -158,3 +158,30 @@ def test_linear_batch_pair_copies_follow_volume_updates(tmp_path, monkeypatch):
     torch.cuda.synchronize()
     _per_call_equal(reqs, "linear")
     batch.close()
+
+
+def test_linear_batch_scaled_and_curved_match_per_call(tmp_path, monkeypatch):
+    """Scaled requests and the Ewald curvature go through the batch's pair copies too (coordinates by
+    the same slice2grid): results are the per-call ones, bit for bit."""
+    import torch
+    from noa_b200 import fourier_project as fp
+    from noa_b200 import synthetic
+    from noa_b200.batch import ExtractBatch
+    monkeypatch.setenv("NB_AUTOTUNE_CACHE", str(tmp_path / "autotune.txt"))
+    reqs, _ = _large_requests([(64, 300), (48, 400)], seed=13)
+    for i, r in enumerate(reqs):
+        count = r.slice_shape[0]
+        sc = synthetic.scale_matrices(count, (1.0, 1.0), seed=80 + i, jitter=0.05).astype(np.float32)
+        r.inv_scaling = torch.from_numpy(sc).cuda()
+    ews = (45.0, 60.0)
+    batch = ExtractBatch("hc2h", reqs, interp="linear", ews_radius=ews, autotune=False)
+    batch.run()
+    torch.cuda.synchronize()
+    for r in reqs:
+        count, n = r.slice_shape[0], r.slice_shape[2]
+        ref = torch.zeros((count, 1, n, n // 2 + 1), dtype=torch.complex64, device="cuda")
+        fp.extract_central_slices_3d("hc2h", r.volume, None, r.volume_shape, ref, None, r.slice_shape, r.inv_scaling,
+                                     r.fwd_rotation, interp="linear", ews_radius=ews)
+        torch.cuda.synchronize()
+        assert torch.equal(r.slice, ref)
+    batch.close()
