@@ -473,8 +473,10 @@ struct View3 {
 __device__ __forceinline__ float4 ldg_evict_last_half(const float4* p) {
     unsigned long long pol;
     asm("createpolicy.fractional.L2::evict_last.b64 %0, 0.5;" : "=l"(pol));
+    // The policy touches no memory and may be hoisted; the load is volatile so that it is never
+    // speculated above the bounds tests that guard it (a tap's address is only valid when they pass).
     float4 v;
-    asm("ld.global.nc.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+    asm volatile("ld.global.nc.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
                  : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(p), "l"(pol));
     return v;
 }
