@@ -5,8 +5,10 @@
 // twice: slice i can only contribute to a pixel whose 3-D frequency g satisfies |n_i . g| < blackman,
 // and without curvature g is linear in the pixel's 2-D frequency, so n_i . g over a box of pixels is an
 // interval known from two dot products (patch_reaches). The slices whose interval over the CTA's box
-// meets the slab are compacted, in increasing order, into shared memory; each warp re-tests that list
-// against its own box (one candidate per lane) and walks the survivors' ballot in lane order.
+// meets the slab are compacted, in increasing order, into shared memory, 4096 at a time, each warp
+// compacting its own range of slice indices so that building the list needs no barrier; each warp then
+// re-tests the whole list against its own box (one candidate per lane) and walks the survivors' ballot
+// in lane order, with no barrier until the next pass.
 // Summation order per pixel is therefore the reference's (increasing slice index). With an Ewald
 // sphere (curved slices) nothing is culled. The w-windowed form sums the w offsets in registers (in w order)
 // rather than zero-filling and adding atomically; each offset re-samples the virtual volume at the
@@ -18,6 +20,8 @@ namespace {
 
 constexpr int IE_THREADS = 256;
 constexpr int IE_TILE = 16;  // 16x16 pixels per CTA; warps own 4x8 sub-tiles
+constexpr int IE_LIST = 4096;                           // input slices culled per pass (16 KB of indices)
+constexpr int IE_REGION = IE_LIST / (IE_THREADS / 32);  // of which each warp compacts one range
 
 // A box of 2-D output frequencies: centre and half-extent per axis.
 struct Box2 {
@@ -46,9 +50,8 @@ __device__ __forceinline__ bool patch_reaches(const float3 n, const Patch& p, co
 template<int I, bool IN_C, bool OUT_C>
 __global__ void __launch_bounds__(IE_THREADS)
 insert_extract_kernel(const __grid_constant__ ProjArgs a, int ntx, int tiles_per_slice, int64_t n_tiles) {
-    __shared__ int s_list[IE_THREADS];
+    __shared__ int s_list[IE_LIST];
     __shared__ int s_warp_count[IE_THREADS / 32];
-    __shared__ int s_count;
     __shared__ float s_box[4][IE_THREADS / 32];
 
     const int wp = a.slice_w / 2 + 1;
@@ -122,47 +125,50 @@ insert_extract_kernel(const __grid_constant__ ProjArgs a, int ntx, int tiles_per
             float2 value = make_float2(0.f, 0.f);
             float weight = 0.f;
 
-            for (int64_t chunk = 0; chunk < a.n_in; chunk += IE_THREADS) {
-                const int64_t i = chunk + tid;
-                bool keep = false;
-                if (i < a.n_in)
-                    keep = !cull || patch_reaches(rotation_row0(a.rot, i), patch, cbox, off, a.fb);
-                const unsigned ballot = __ballot_sync(0xffffffffu, keep);
+            for (int64_t super = 0; super < a.n_in; super += IE_LIST) {
+                int cnt = 0;
+                for (int r = 0; r < IE_REGION; r += 32) {
+                    const int64_t i = super + warp * IE_REGION + r + lane;
+                    if (super + warp * IE_REGION + r >= a.n_in)
+                        break;
+                    const bool keep = i < a.n_in &&
+                                      (!cull || patch_reaches(rotation_row0(a.rot, i), patch, cbox, off, a.fb));
+                    const unsigned ballot = __ballot_sync(0xffffffffu, keep);
+                    if (keep)
+                        s_list[warp * IE_REGION + cnt + __popc(ballot & ((1u << lane) - 1u))] =
+                            static_cast<int>(i - super);
+                    cnt += __popc(ballot);
+                }
                 if (lane == 0)
-                    s_warp_count[warp] = __popc(ballot);
+                    s_warp_count[warp] = cnt;
                 __syncthreads();
-                int base = 0;
-                for (int k = 0; k < warp; ++k)
-                    base += s_warp_count[k];
-                if (keep)
-                    s_list[base + __popc(ballot & ((1u << lane) - 1u))] = static_cast<int>(i - chunk);
-                if (tid == IE_THREADS - 1)
-                    s_count = base + __popc(ballot);
-                __syncthreads();
-                const int count = s_count;
-                // Warp-uniform loops: the list, the ballot and warp_valid are the same in every lane.
-                for (int g = 0; warp_valid && g < count; g += 32) {
-                    const int k = g + lane;
-                    const bool wkeep = k < count &&
-                                       (!cull || patch_reaches(rotation_row0(a.rot, chunk + s_list[k]), patch, wbox,
-                                                               off, a.fb));
-                    unsigned todo = __ballot_sync(0xffffffffu, wkeep);
-                    while (todo) {
-                        const int j = __ffs(todo) - 1;
-                        todo &= todo - 1u;
-                        if (!in_cut)
-                            continue;
-                        const int64_t si = chunk + s_list[g + j];
-                        float f0, f1;
-                        const float fz = grid2slice(sz, gy, gx, a.scale, a.rot, si, a.ews, f0, f1);
-                        if (fabsf(fz) < a.fb) {
-                            const float ws = windowed_sinc_fast(fz, a.pfs, a.pfb);
-                            const float q0 = mul(f0, a.f_in0), q1 = mul(f1, a.f_in1);
-                            value = cadd(value, cmul(interp_spectrum_2d<I, IN_C>(a.in, sp, si, q0, q1), ws));
-                            if (has_in_w)
-                                weight = add(weight, mul(interp_spectrum_2d<I, false>(a.in_w, sp, si, q0, q1).x, ws));
-                            else
-                                weight = add(weight, ws);
+                for (int region = 0; warp_valid && region < IE_THREADS / 32; ++region) {
+                    const int count = s_warp_count[region];
+                    const int* list = s_list + region * IE_REGION;
+                    for (int g = 0; g < count; g += 32) {
+                        const int k = g + lane;
+                        const bool wkeep = k < count &&
+                                           (!cull || patch_reaches(rotation_row0(a.rot, super + list[k]), patch, wbox,
+                                                                   off, a.fb));
+                        unsigned todo = __ballot_sync(0xffffffffu, wkeep);
+                        while (todo) {
+                            const int j = __ffs(todo) - 1;
+                            todo &= todo - 1u;
+                            if (!in_cut)
+                                continue;
+                            const int64_t si = super + list[g + j];
+                            float f0, f1;
+                            const float fz = grid2slice(sz, gy, gx, a.scale, a.rot, si, a.ews, f0, f1);
+                            if (fabsf(fz) < a.fb) {
+                                const float ws = windowed_sinc_fast(fz, a.pfs, a.pfb);
+                                const float q0 = mul(f0, a.f_in0), q1 = mul(f1, a.f_in1);
+                                value = cadd(value, cmul(interp_spectrum_2d<I, IN_C>(a.in, sp, si, q0, q1), ws));
+                                if (has_in_w)
+                                    weight = add(weight,
+                                                 mul(interp_spectrum_2d<I, false>(a.in_w, sp, si, q0, q1).x, ws));
+                                else
+                                    weight = add(weight, ws);
+                            }
                         }
                     }
                 }
