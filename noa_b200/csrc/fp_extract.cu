@@ -27,6 +27,24 @@ constexpr int TY = 16, TX = 16, EXTRACT_THREADS = TY * TX;
 // ---------------------------------------------------------------------------------------------------
 constexpr int PAIR_PPT = 4;
 
+// The w-window's values depend on the offset alone, so a CTA tabulates them once (the same expression
+// as the per-sample one, hence the same bits) instead of evaluating the window for every pixel and
+// offset. Windows of more than W_TABLE offsets evaluate the rest per sample.
+constexpr int W_TABLE = 64;
+
+// Called by every thread of the CTA before any of them returns (it synchronizes when wsize > 1).
+__device__ __forceinline__ void fill_w_table(const ProjArgs& a, float* table) {
+    if (a.wsize <= 1)
+        return;
+    for (int w = threadIdx.x; w < a.wsize && w < W_TABLE; w += blockDim.x)
+        table[w] = windowed_sinc(div(static_cast<float>(w - a.wsize / 2), a.target0), a.efs, a.efb);
+    __syncthreads();
+}
+
+__device__ __forceinline__ float w_value(const ProjArgs& a, const float* table, int w, float off) {
+    return w < W_TABLE ? table[w] : windowed_sinc(off, a.efs, a.efb);
+}
+
 __global__ void make_pairs(const __grid_constant__ ProjArgs a, float4* __restrict__ pairs) {
     const int D = a.vol_d, H = a.vol_h, WP = a.vol_w / 2 + 1;
     const int64_t n = static_cast<int64_t>(D) * H * WP;
@@ -97,6 +115,8 @@ extract_pairs_w_kernel(const __grid_constant__ ProjArgs a, const float4* __restr
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int y0 = (blockIdx.x / ntx) * (TY * PAIR_PPT) + (warp >> 1) * 4 + (lane >> 3);
     const int u = (blockIdx.x % ntx) * TX + (warp & 1) * 8 + (lane & 7);
+    __shared__ float s_w[W_TABLE];
+    fill_w_table(a, s_w);
     if (u >= wp)
         return;
     const Spectrum3 sp{a.vol_d, a.vol_h, a.vol_w, a.in_centered};
@@ -121,7 +141,7 @@ extract_pairs_w_kernel(const __grid_constant__ ProjArgs a, const float4* __restr
                 const float gz = add(fz, off);
                 if (dot3(gz, fy, fx, gz, fy, fx) > a.cutoff_sqd)
                     continue;
-                const float cw = windowed_sinc(off, a.efs, a.efb);
+                const float cw = w_value(a, s_w, w, off);
                 const float2 iv = to_output<true, OUT_C>(interp_linear_pairs(
                     pairs, sz, sy, sp, mul(gz, a.target0), mul(fy, a.target1), mul(fx, a.target2)));
                 value = cadd(value, cmul(iv, cw));
@@ -179,6 +199,8 @@ extract_kernel(const __grid_constant__ ProjArgs a, int ntx) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int y = (blockIdx.x / ntx) * TY + (warp >> 1) * 4 + (lane >> 3);
     const int u = (blockIdx.x % ntx) * TX + (warp & 1) * 8 + (lane & 7);
+    __shared__ float s_w[W_TABLE];
+    fill_w_table(a, s_w);
     if (u >= wp || y >= a.slice_h)
         return;
     const Spectrum3 sp{a.vol_d, a.vol_h, a.vol_w, a.in_centered};
@@ -211,7 +233,7 @@ extract_kernel(const __grid_constant__ ProjArgs a, int ntx) {
                 if (dot3(gz, fy, fx, gz, fy, fx) > a.cutoff_sqd)
                     continue;
                 const float q0 = mul(gz, a.target0), q1 = mul(fy, a.target1), q2 = mul(fx, a.target2);
-                const float cw = windowed_sinc(off, a.efs, a.efb);
+                const float cw = w_value(a, s_w, w, off);
                 const float2 iv = to_output<IN_C, OUT_C>(interp_3d<I, IN_C>(vol, sp, q0, q1, q2));
                 value = cadd(value, cmul(iv, cw));
                 if (has_out_w) {
