@@ -237,10 +237,11 @@ batch_extract_kernel(const BatchReq* __restrict__ reqs, int n_req, int64_t n_ite
     }
 }
 
-// Pairs-only batches of at most PACK requests pass their descriptors as a kernel parameter: the
+// Pairs-only batch graphs of at most PACK requests pass their descriptors as a kernel parameter: the
 // request fields are then read through the constant bank like a per-call kernel's arguments, with no
 // staging in shared memory and no barrier when a CTA's request changes (28.4 KB of parameters, within
-// the 32 KB that sm_70+ kernels accept).
+// the 32 KB that sm_70+ kernels accept). Only captured graphs use it, where the parameters are set
+// once: one-shot launches keep the shared-memory descriptors.
 constexpr int PACK = 48;
 struct ReqPack { BatchReq r[PACK]; };
 static_assert(sizeof(ReqPack) + 64 <= 32764, "the descriptor pack must fit the kernel parameter space");
