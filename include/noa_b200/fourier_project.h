@@ -160,17 +160,36 @@ NB_API int nb_insert_and_extract_central_slices_3d(
  * nb_rasterize_central_slices_3d, but the call allocates no device memory: for callers that cannot let
  * a library allocate at call time (a fixed up-front memory budget, an allocator owned by someone else,
  * a steady state that must not enter the driver's allocator). With output weights, the (value, weight)
- * accumulator lives in a 64 MiB array this library reserves on every GPU that loads it, until exit, so
- * the rfft grid D*H*(W/2+1) may hold at most 4,194,304 voxels for complex values (8,388,608 for real
- * ones); larger volumes return NB_ERROR_INVALID. The first call on a device looks the array up (make
- * it before any stream capture). All calls share the array and each clears the part it uses first:
- * calls that overlap on the GPU race, so order them. */
+ * accumulator lives in a 64 MiB array of this library's device code. CUDA reserves it on a GPU when it
+ * loads that code there: by default (lazy module loading) during the first call on that GPU, or when the
+ * library loads under CUDA_MODULE_LOADING=EAGER; it is then held until exit. So make one warm-up call
+ * per GPU while setting up a memory budget (and before any stream capture: the first call also looks
+ * the array's address up); the calls after it allocate nothing. The rfft grid D*H*(W/2+1) may hold at
+ * most 4,194,304 voxels for complex values (8,388,608 for real ones); larger volumes return
+ * NB_ERROR_INVALID. All calls share the array and each clears the part it uses first: calls that
+ * overlap on the GPU race, so order them. */
 NB_API int nb_rasterize_central_slices_3d_static_scratch(
     int32_t remap,
     const nb_array* slice, const nb_array* slice_weight, const int64_t slice_shape[4],
     const nb_array* volume, const nb_array* volume_weight, const int64_t volume_shape[4],
     const nb_transform* inv_scaling, const nb_transform* fwd_rotation,
     const nb_options* options, void* stream);
+
+/* No counterpart in the reference (noa's Array allocations are the caller's). Caps the size of any
+ * ONE device allocation this library makes on its own behalf on CUDA device `device`: the per-call
+ * scratch of the fast paths (the pair copy of a LINEAR extraction, 16 bytes per rfft voxel; the padded
+ * accumulator of a rasterization or scatter insertion, up to 16 bytes per voxel of the grid padded to
+ * the cutoff; a one-shot batched launch's descriptors) and a captured batch's descriptors and pair
+ * copies. An allocation above the cap fails as if the device were out of memory, so calls take their
+ * path without it, with the same results: extraction reads the volume directly, rasterization reduces
+ * into an unpadded scratch or straight into the caller's grids, the scatter insertion runs the gather
+ * form; a batch whose descriptors cannot be allocated returns NB_ERROR_OOM. bytes < 0 removes the cap
+ * (the default); 0 makes every call take its path without scratch. Applies to calls made after it
+ * returns, from any thread. NB_ERROR_INVALID for a device that does not exist. */
+NB_API int nb_set_scratch_limit(int32_t device, int64_t bytes);
+
+/* The cap set on `device` in bytes, -1 when there is none (or the device does not exist). */
+NB_API int64_t nb_scratch_limit(int32_t device);
 
 /* Description of the last error on the calling thread ("" if none). */
 NB_API const char* nb_last_error(void);

@@ -8,10 +8,12 @@
 // reference's f32 coordinate type.
 #include "fp_args.cuh"
 #include "fp_pairs.cuh"
+#include "fp_pool.cuh"
 
 #include "noa_b200/batch.h"
 #include "noa_b200/fourier_project.h"
 
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -20,17 +22,19 @@
 namespace nb {
 
 int sm_count() {
-    static int counts[64] = {};
+    // Filled on first use per device; concurrent first calls store the same value.
+    static std::atomic<int> counts[64];
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64)
         dev = 0;
-    if (counts[dev] == 0) {
-        int n = 0;
+    int n = counts[dev].load(std::memory_order_relaxed);
+    if (n == 0) {
         cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-        counts[dev] = n > 0 ? n : 148;
+        n = n > 0 ? n : 148;
+        counts[dev].store(n, std::memory_order_relaxed);
     }
-    return counts[dev];
+    return n;
 }
 
 namespace {
@@ -454,6 +458,7 @@ int prepare_insert(
     a.fb = fmax_ref(static_cast<float>(options->fftfreq_blackman), 1.f / tmin);
     a.pfs = static_cast<float>(3.14159265358979323846 / static_cast<double>(a.fs));
     a.pfb = static_cast<float>(3.14159265358979323846 / static_cast<double>(a.fb));
+    a.ifs = static_cast<float>(1.0 / static_cast<double>(a.fs));
     a.in_slice_narrow = slice_narrow(slice) && (!is_array(slice_weight) || slice_narrow(slice_weight));
     a.in_cplx = is_complex(slice->dtype);
     a.out_cplx = is_complex(volume->dtype);
@@ -618,6 +623,19 @@ const char* nb_last_error(void) { return g_last_error.c_str(); }
 
 const char* nb_version(void) { return "0.1.0"; }
 
+int nb_set_scratch_limit(int32_t device, int64_t bytes) {
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess) {
+        cudaGetLastError();
+        count = 0;
+    }
+    if (device < 0 || device >= count || !nb::set_scratch_limit(device, bytes))
+        return nb::report_error(NB_ERROR_INVALID, "no such device");
+    return NB_OK;
+}
+
+int64_t nb_scratch_limit(int32_t device) { return nb::scratch_limit(device); }
+
 int nb_rasterize_central_slices_3d(
     int32_t remap,
     const nb_array* slice, const nb_array* slice_weight, const int64_t slice_shape[4],
@@ -724,6 +742,7 @@ int nb_insert_and_extract_central_slices_3d(
     a.fb = fmax_ref(static_cast<float>(options->fftfreq_blackman), 1.f / vz);
     a.pfs = static_cast<float>(3.14159265358979323846 / static_cast<double>(a.fs));
     a.pfb = static_cast<float>(3.14159265358979323846 / static_cast<double>(a.fb));
+    a.ifs = static_cast<float>(1.0 / static_cast<double>(a.fs));
     a.efs = fmax_ref(static_cast<float>(options->w_fftfreq_sinc), 1.f / vz);
     a.efb = fmax_ref(static_cast<float>(options->w_fftfreq_blackman), 1.f / vz);
     a.wsize = blackman_window_size(a.efb, vz);

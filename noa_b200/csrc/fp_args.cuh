@@ -31,6 +31,7 @@ struct ProjArgs {
     float cutoff_sqd;
     float fs, fb;              // windowed sinc (insert; insert_extract input)
     float pfs, pfb;            // pi / fs, pi / fb (for windowed_sinc_fast)
+    float ifs;                 // 1 / fs (the sinc phase in units of pi, for sinpif)
     float efs, efb;            // w-windowed sinc (extract; insert_extract output)
     int wsize;                 // w-window size (1 = plain 3-D form)
     float vz;                  // insert_extract: the virtual volume's z size

@@ -575,11 +575,9 @@ void plan_pairs(nb_extract_batch_t* h) {
         const int64_t vox = static_cast<int64_t>(v.a->vol_d) * v.a->vol_h * (v.a->vol_w / 2 + 1);
         if (v.pixels < 2 * vox)
             continue;
-        float4* buf = nullptr;
-        if (cudaMalloc(&buf, static_cast<size_t>(vox) * sizeof(float4)) != cudaSuccess) {
-            cudaGetLastError();
-            continue;
-        }
+        float4* buf = static_cast<float4*>(device_alloc(static_cast<size_t>(vox) * sizeof(float4)));
+        if (!buf)
+            continue;  // no memory for the copy: these requests read the volume itself
         h->pair_jobs.push_back({*v.a, buf});
         for (size_t i : v.reqs)
             h->host_reqs[i].pairs = buf;
@@ -691,9 +689,9 @@ int nb_extract_batch_create(int32_t remap, const nb_extract_request* requests, i
         h->host_reqs[static_cast<size_t>(i)].pairs = nullptr;
     }
     plan_pairs(h);
-    if (cudaMalloc(&h->d_reqs, h->host_reqs.size() * sizeof(BatchReq)) != cudaSuccess ||
-        cudaMalloc(&h->d_counter, sizeof(unsigned long long)) != cudaSuccess) {
-        cudaGetLastError();
+    h->d_reqs = static_cast<BatchReq*>(device_alloc(h->host_reqs.size() * sizeof(BatchReq)));
+    h->d_counter = static_cast<unsigned long long*>(h->d_reqs ? device_alloc(sizeof(unsigned long long)) : nullptr);
+    if (!h->d_reqs || !h->d_counter) {
         release(h);
         return report_error(NB_ERROR_OOM, "cannot allocate the batch descriptors");
     }

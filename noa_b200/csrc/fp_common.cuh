@@ -206,13 +206,16 @@ __device__ __forceinline__ float windowed_sinc(float fftfreq, float fftfreq_sinc
 // stays within [-pi, pi], is the hardware approximation __cosf (6-10 % faster insertions). The sinc's
 // sine is not __sinf: its argument reaches several pi, where __sinf's error grew the insertions' error
 // to 1e-4. Relative difference from windowed_sinc: a few 1e-7.
-// SINPI: the sinc's sine as sinpif(xs / pi) (argument reduction by rounding) rather than sinf(xs):
-// 8.5 % faster in the gather insertion and 5.5 % in insert_and_extract, 11 % slower in the scatter
-// form (each measured in one call), so those two use it; the two forms differ by 2e-7 (relative L2).
+// SINPI: the sinc's sine as sinpif(fftfreq * (1 / fftfreq_sinc)) rather than sinf(xs): 8.5 % faster in
+// the gather insertion and 5.5 % in insert_and_extract, 11 % slower in the scatter form (each measured
+// in one call), so those two use it; the two forms differ by 2e-7 (relative L2). sinpif's argument is
+// the sinc's phase in units of pi, rounded twice (the reciprocal, then the product), and xs only feeds
+// the division.
 template<bool SINPI = false>
-__device__ __forceinline__ float windowed_sinc_fast(float fftfreq, float pi_over_sinc, float pi_over_blackman) {
+__device__ __forceinline__ float windowed_sinc_fast(float fftfreq, float pi_over_sinc, float inv_sinc,
+                                                    float pi_over_blackman) {
     const float xs = fftfreq * pi_over_sinc;
-    const float sn = SINPI ? sinpif(xs * 0.318309886183790672f) : sinf(xs);
+    const float sn = SINPI ? sinpif(fftfreq * inv_sinc) : sinf(xs);
     const float sinc = xs == 0.f ? 1.f : __fdividef(sn, xs);
     const float c = __cosf(fftfreq * pi_over_blackman);
     const float blackman = 0.42f + 0.5f * c + 0.08f * (2.f * c * c - 1.f);

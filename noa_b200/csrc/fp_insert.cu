@@ -117,7 +117,7 @@ insert_kernel(const __grid_constant__ ProjArgs a, int nbz, int nby, int nbx) {
                     float f0, f1;
                     const float zz = grid2slice(fz, fy, fx, a.scale, a.rot, si, a.ews, f0, f1);
                     if (fabsf(zz) <= a.fb) {
-                        const float window = windowed_sinc_fast<true>(zz, a.pfs, a.pfb);
+                        const float window = windowed_sinc_fast<true>(zz, a.pfs, a.ifs, a.pfb);
                         const float q0 = mul(f0, a.f_slice0), q1 = mul(f1, a.f_slice1);
                         value = cadd(value, cmul(interp_spectrum_2d<I, IN_C>(a.in, sp, si, q0, q1), window));
                         if (has_out_w) {

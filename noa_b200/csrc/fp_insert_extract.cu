@@ -160,7 +160,7 @@ insert_extract_kernel(const __grid_constant__ ProjArgs a, int ntx, int tiles_per
                             float f0, f1;
                             const float fz = grid2slice(sz, gy, gx, a.scale, a.rot, si, a.ews, f0, f1);
                             if (fabsf(fz) < a.fb) {
-                                const float ws = windowed_sinc_fast<true>(fz, a.pfs, a.pfb);
+                                const float ws = windowed_sinc_fast<true>(fz, a.pfs, a.ifs, a.pfb);
                                 const float q0 = mul(f0, a.f_in0), q1 = mul(f1, a.f_in1);
                                 value = cadd(value, cmul(interp_spectrum_2d<I, IN_C>(a.in, sp, si, q0, q1), ws));
                                 if (has_in_w)

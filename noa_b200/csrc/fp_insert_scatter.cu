@@ -94,7 +94,7 @@ insert_scatter_kernel(const __grid_constant__ ProjArgs a, void* __restrict__ acc
             const float zz = grid2slice(fz, fy, fx, a.scale, a.rot, i, a.ews, f0, f1);
             if (!(fabsf(zz) <= a.fb))
                 continue;
-            const float window = windowed_sinc_fast(zz, a.pfs, a.pfb);
+            const float window = windowed_sinc_fast(zz, a.pfs, a.ifs, a.pfb);
             const float q0 = mul(f0, a.f_slice0), q1 = mul(f1, a.f_slice1);
             const float2 v = cmul(interp_spectrum_2d<I, IN_C>(a.in, sp, i, q0, q1), window);
             float w = 0.f;

@@ -1,16 +1,29 @@
-// Stream-ordered scratch allocations for the kernels that stage data (volume pair copy for extraction,
-// interleaved accumulator for rasterization): one CUDA memory pool per device, created on first use
-// with a release threshold that keeps freed blocks for reuse, so steady-state calls do not go back to
-// the driver.
+// Device memory this library allocates on its own behalf:
+//  * stream-ordered scratch for the kernels that stage data (volume pair copy for extraction,
+//    interleaved accumulator for rasterization and the scatter insertion, batch descriptors of one-shot
+//    launches): one CUDA memory pool per device, created on first use with a release threshold that
+//    keeps freed blocks for reuse, so steady-state calls do not go back to the driver;
+//  * the long-lived buffers of a captured batch (descriptors, pair copies), from cudaMalloc.
+// Both go through a per-device cap on the size of one allocation (nb_set_scratch_limit): a request
+// above it fails as if the device were out of memory, and the caller takes its path without it.
 #pragma once
 
+#include <cstddef>
+#include <cstdint>
 #include <cuda_runtime.h>
 
 namespace nb {
 
 // Allocates `bytes` on `stream` from this library's pool of the current device; nullptr on failure
-// (the CUDA error is cleared: callers fall back to a path without scratch).
+// or above the device's cap (the CUDA error is cleared: callers fall back to a path without scratch).
 void* scratch_alloc(size_t bytes, cudaStream_t stream);
 void scratch_free(void* ptr, cudaStream_t stream);
+
+// cudaMalloc on the current device under the same cap; nullptr on failure (error cleared).
+void* device_alloc(size_t bytes);
+
+// The cap of `device` in bytes (-1: none). Setting a negative value removes it.
+bool set_scratch_limit(int device, int64_t bytes);
+int64_t scratch_limit(int device);
 
 } // namespace nb

@@ -1,6 +1,5 @@
 // nb_rasterize_central_slices_3d_static_scratch: the rasterization of nb_rasterize_central_slices_3d
-// with its accumulator in memory this library reserves when it is loaded, so the call allocates
-// nothing.
+// with its accumulator in a fixed array of this library's device code, so the call allocates nothing.
 //
 // Why: the regular entry point takes its interleaved (value, weight) accumulator from a stream-ordered
 // memory pool on every call. Some callers cannot let a library allocate device memory at call time:
@@ -9,8 +8,12 @@
 // driver's allocator in its steady state. This entry point serves them.
 //
 // Limits and rules:
-//   * The accumulator is a file-scope __device__ array of STATIC_SCRATCH_BYTES (64 MiB), held on
-//     every GPU that loads this library until the process exits. With output weights, volumes up to
+//   * The accumulator is a file-scope __device__ array of STATIC_SCRATCH_BYTES (64 MiB). CUDA reserves
+//     it on a GPU when it loads this file's module there: with the default lazy module loading, during
+//     the first call on that GPU (the address lookup below loads it), or when the library is loaded
+//     with CUDA_MODULE_LOADING=EAGER. From then on it is held until the process exits. So a caller
+//     with a fixed memory budget makes one warm-up call per GPU while it sets that budget up; later
+//     calls allocate nothing. With output weights, volumes up to
 //     STATIC_SCRATCH_BYTES / 16 voxels (complex values) or / 8 voxels (real values) of the rfft grid
 //     (D * H * (W/2+1)) are accepted; larger volumes are rejected with NB_ERROR_INVALID. Without output
 //     weights the reductions go straight into the caller's grid and no scratch is used at all.

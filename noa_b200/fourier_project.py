@@ -87,6 +87,10 @@ def lib() -> C.CDLL:
         h.nb_last_error.restype = C.c_char_p
         h.nb_version.restype = C.c_char_p
         h.nb_options_default.argtypes = [opt]
+        h.nb_set_scratch_limit.argtypes = [C.c_int32, C.c_int64]
+        h.nb_set_scratch_limit.restype = C.c_int
+        h.nb_scratch_limit.argtypes = [C.c_int32]
+        h.nb_scratch_limit.restype = C.c_int64
         _lib_handle = h
     return _lib_handle
 
@@ -347,3 +351,26 @@ def insert_and_extract_central_slices_3d(remap: str, input_slice, input_weight, 
 
 def version() -> str:
     return lib().nb_version().decode()
+
+
+def _device_index(device) -> int:
+    if device is None:
+        return _torch().cuda.current_device()
+    if isinstance(device, int):
+        return device
+    d = _torch().device(device)
+    return d.index if d.index is not None else _torch().cuda.current_device()
+
+
+def set_scratch_limit(nbytes: int | None, device=None) -> None:
+    """Caps the size of any one device allocation the library makes on its own on ``device`` (default:
+    the current CUDA device): the fast paths' scratch (pair copies, padded accumulators) and batch
+    buffers. Calls then take their paths without that memory, with the same results; batched launches
+    that cannot allocate their descriptors raise NB_ERROR_OOM. ``None`` removes the cap."""
+    _check(lib().nb_set_scratch_limit(_device_index(device), -1 if nbytes is None else int(nbytes)))
+
+
+def scratch_limit(device=None) -> int | None:
+    """The cap set with ``set_scratch_limit`` (None when there is none)."""
+    v = int(lib().nb_scratch_limit(_device_index(device)))
+    return None if v < 0 else v

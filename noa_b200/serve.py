@@ -14,6 +14,13 @@ their slices). ``ProjectionServer.poll()`` runs one scheduling round:
    queued there; admitted insertions each get a rasterization into their own zeroed value + weight
    accumulator on one of the insertion streams, round robin.
 
+Backpressure and cancellation: with ``max_waiting`` set, ``submit()`` refuses a request while that many
+wait for admission (it raises ``ServerBusy``; the client keeps the request and offers it again, as
+``run_stream`` does), so the queue and the host memory it pins stay bounded under overload.
+``cancel()`` withdraws a request that has not been launched yet (waiting, or an admitted extraction
+not yet packed into a batch, whose memory returns to the budget); work already on the device cannot be
+recalled, so such a request completes normally.
+
 Continuous batching: extractions that arrive while a batch runs are admitted as memory frees up and
 form the next batch, which is already queued behind the running one, so the device never waits for
 the host; insertions run concurrently on their own streams. The scheduling logic is independent of
@@ -229,11 +236,17 @@ class CudaExecutor(Executor):
             s.synchronize()
 
 
+class ServerBusy(RuntimeError):
+    """``submit()`` refused a request because ``max_waiting`` requests already wait for admission."""
+
+
 @dataclass
 class ServerStats:
     submitted: int = 0
     completed: int = 0
     rejected: int = 0
+    refused: int = 0         # submit() calls turned away by backpressure (the client may retry)
+    cancelled: int = 0
     batches: int = 0
     batch_requests: int = 0
     batch_slices: int = 0
@@ -247,12 +260,16 @@ class ProjectionServer:
     """Admission by device-memory budget and continuous batching (see the module docstring).
 
     ``budget_bytes`` caps resident volumes plus admitted requests. ``keep_outputs=False`` drops each
-    request's outputs when it completes (a benchmark's client), else they stay on the request."""
+    request's outputs when it completes (a benchmark's client), else they stay on the request.
+    ``max_waiting`` (None: unbounded) is the length of the admission queue beyond which ``submit()``
+    raises ``ServerBusy``."""
 
     def __init__(self, executor: Executor, budget_bytes: int, *, max_batch_slices=65536,
-                 max_inflight_batches=2, keep_outputs=True, clock=time.perf_counter):
+                 max_inflight_batches=2, keep_outputs=True, max_waiting: int | None = None,
+                 clock=time.perf_counter):
         self.ex = executor
         self.budget = int(budget_bytes)
+        self.max_waiting = None if max_waiting is None else int(max_waiting)
         self.max_batch_slices = int(max_batch_slices)
         self.max_inflight_batches = int(max_inflight_batches)
         self.keep_outputs = keep_outputs
@@ -298,6 +315,9 @@ class ProjectionServer:
             raise ValueError(f"unknown request kind {req.kind!r}")
         if req.volume_id not in self.volumes:
             raise KeyError(f"volume {req.volume_id} is not resident")
+        if self.max_waiting is not None and len(self.waiting) >= self.max_waiting:
+            self.stats.refused += 1
+            raise ServerBusy(f"{len(self.waiting)} requests wait for admission (max_waiting={self.max_waiting})")
         if req.rid < 0:
             req.rid = self._rid
         self._rid += 1
@@ -305,6 +325,24 @@ class ProjectionServer:
         self.stats.submitted += 1
         self.stats.max_waiting = max(self.stats.max_waiting, len(self.waiting))
         return req
+
+    def cancel(self, req: Request) -> bool:
+        """Withdraws ``req`` if it has not been launched: it leaves the admission queue, or, for an
+        admitted extraction not yet in a batch, the launch queue (its memory returns to the budget).
+        Returns True then, with ``req.error == "cancelled"``. Returns False for a request already on the
+        device (it completes normally: its work cannot be recalled from the GPU), finished, or unknown."""
+        for queue, admitted in ((self.waiting, False), (self.ready_extract, True)):
+            for i, r in enumerate(queue):
+                if r is req:
+                    del queue[i]
+                    if admitted:
+                        self.used -= footprint(r, self.volumes[r.volume_id].box)
+                    r.error = "cancelled"
+                    r.done = self.clock()
+                    r.keep.clear()
+                    self.stats.cancelled += 1
+                    return True
+        return False
 
     def busy(self) -> bool:
         return bool(self.waiting or self.ready_extract or self.inflight)
@@ -405,8 +443,9 @@ def latency_summary(reqs: list[Request]) -> dict:
 def run_stream(server: ProjectionServer, requests: list[Request], *, clock=time.perf_counter,
                idle_sleep=5e-5) -> tuple[float, float]:
     """Feeds ``requests`` (sorted by ``arrival``, seconds from the start) to the server in real time and
-    polls it until every request is finished. Arrival times are rebased onto ``clock``. Returns the
-    (start, end) clock values."""
+    polls it until every request is finished. Arrival times are rebased onto ``clock``. A request the
+    server refuses (``ServerBusy``) is offered again after the next poll, its latency still counted from
+    its arrival. Returns the (start, end) clock values."""
     t0 = clock()
     for r in requests:
         r.arrival = t0 + r.arrival
@@ -414,7 +453,10 @@ def run_stream(server: ProjectionServer, requests: list[Request], *, clock=time.
     while i < len(requests) or server.busy():
         now = clock()
         while i < len(requests) and requests[i].arrival <= now:
-            server.submit(requests[i])
+            try:
+                server.submit(requests[i])
+            except ServerBusy:
+                break  # backpressure: offer it again after the next scheduling round
             i += 1
         server.poll()
         if not server.busy() and i < len(requests):

@@ -7,7 +7,8 @@ checked deterministically.
 import numpy as np
 import pytest
 
-from noa_b200.serve import Executor, ProjectionServer, Request, footprint, latency_summary, run_stream
+from noa_b200.serve import (Executor, ProjectionServer, Request, ServerBusy, footprint, latency_summary,
+                            run_stream)
 
 
 class Clock:
@@ -224,3 +225,63 @@ def test_add_volume_file_reads_an_mrc_rfft_volume(tmp_path):
     assert v.shape == (1, 8, 8, 8) and torch.equal(v.data, torch.from_numpy(vol))
     with pytest.raises(ValueError):
         s.add_volume_file(4, p, logical_width=10)
+
+
+def test_backpressure_refuses_beyond_max_waiting_and_recovers():
+    box = 32
+    one = footprint(Request("extract", 0, rot(100)), box)
+    s, ex, clock = make_server(one + 1000, box=box, n_volumes=1, max_waiting=2)
+    s.resident = 0
+    a = s.submit(Request("extract", 0, rot(100)))
+    s.poll()  # a admitted and launched; the budget holds one request at a time
+    b = s.submit(Request("extract", 0, rot(100)))
+    c = s.submit(Request("extract", 0, rot(100)))
+    with pytest.raises(ServerBusy):
+        s.submit(Request("extract", 0, rot(100)))
+    assert s.stats.refused == 1 and s.stats.submitted == 3 and len(s.waiting) == 2
+    clock.t = 1.0
+    s.poll()  # a completes, b is admitted: the queue has room again
+    d = s.submit(Request("extract", 0, rot(100)))
+    for t in (2.0, 3.0, 4.0, 5.0):
+        clock.t = t
+        s.poll()
+    assert all(r.error is None and not np.isnan(r.done) for r in (a, b, c, d))
+
+
+def test_run_stream_retries_refused_requests():
+    class Instant(FakeExecutor):
+        def done(self, token):
+            return True
+
+    import time
+    clock = Clock()
+    s = ProjectionServer(Instant(clock), 10 ** 9, max_waiting=1)
+    s.add_volume(0, object(), (1, 16, 16, 16))
+    reqs = [Request("extract", 0, rot(4), arrival=0.0) for _ in range(12)]  # all at once
+    run_stream(s, reqs, clock=time.perf_counter)
+    assert s.stats.completed == 12 and s.stats.refused > 0
+    assert all(r.error is None for r in reqs)
+
+
+def test_cancel_waiting_and_admitted_but_not_running_requests():
+    box = 32
+    one = footprint(Request("extract", 0, rot(100)), box)
+    s, ex, clock = make_server(10 * one, box=box, n_volumes=1, max_inflight_batches=1)
+    s.resident = 0
+    running = s.submit(Request("extract", 0, rot(100)))
+    s.poll()  # launched
+    queued = s.submit(Request("extract", 0, rot(100)))
+    s.poll()  # admitted, waiting for the batch slot
+    assert queued in s.ready_extract and s.used == 2 * one
+    assert s.cancel(queued)
+    assert queued.error == "cancelled" and s.used == one and queued not in s.ready_extract
+    waiting = Request("insert", 0, rot(10))
+    s.waiting.append(waiting)  # not yet admitted
+    assert s.cancel(waiting) and waiting.error == "cancelled" and not s.waiting
+    assert not s.cancel(running)  # on the device: it completes normally
+    assert not s.cancel(queued)   # already cancelled
+    clock.t = 1.0
+    done = s.poll()
+    assert done == [running] and running.error is None
+    assert s.stats.cancelled == 2 and s.used == 0 and not s.busy()
+    assert [l[1] for l in ex.launches] == [[running.rid]]
