@@ -268,6 +268,29 @@ class RefLib(_Lib):
         return status, err.value.decode(errors="replace")
 
 
+def ref_gridding_correction(inp: np.ndarray, out: np.ndarray, post_correction: bool = True,
+                            threads: int = 1) -> tuple[int, str]:
+    """The reference's own fourier_interpolation_correction (oracle/_ref, built with the one-expression
+    patch described in oracle/ref_gridding.cpp) on host arrays of the same precision."""
+    lib = RefLib().lib
+    fn = getattr(lib, f"noaref_gridding_correction_{'f64' if out.dtype == np.float64 else 'f32'}")
+    keep = []
+
+    def arr(a):
+        r = RefArray()
+        r.ptr = a.ctypes.data
+        for i in range(4):
+            r.shape[i] = a.shape[i]
+            r.strides[i] = a.strides[i] // a.itemsize
+        keep.append(a)
+        return r
+
+    a_in, a_out = arr(inp), arr(out)
+    err = C.create_string_buffer(512)
+    status = fn(C.byref(a_in), C.byref(a_out), C.c_int32(int(post_correction)), C.c_int(threads), err, C.c_int(512))
+    return status, err.value.decode(errors="replace")
+
+
 def fp_available() -> bool:
     return os.path.exists(FP_LIB)
 

@@ -6,7 +6,8 @@ Each fixture (one .npz per case) holds a case description, its seeded inputs and
 noa's extract/rasterize/insert/insert_and_extract (compiled from the reference sources into
 oracle/_ref/libnoa_ref.so, run single-threaded). tests/test_oracle.py checks the C restatement
 (oracle/libfp_oracle.so) against these fixtures bit for bit, so the pin holds wherever the reference
-sources are absent.
+sources are absent. The h*_gridding fixtures come from the reference's fourier_interpolation_correction,
+built with the one-expression patch that lets its GriddingCorrection compile (oracle/ref_gridding.cpp).
 """
 from __future__ import annotations
 
@@ -22,7 +23,7 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "tests"))
 
 from cases import build, clone, pin_cases, case_id  # noqa: E402
-from oracle.oracle import RefLib  # noqa: E402
+from oracle.oracle import RefLib, ref_gridding_correction  # noqa: E402
 
 
 def golden_cases() -> list[dict]:
@@ -37,11 +38,37 @@ def golden_cases() -> list[dict]:
     return keep
 
 
+# Gridding correction (fourier_interpolation_correction): shapes with even, odd and size-1 dimensions,
+# a batch, and an input broadcast along the batch; f32 and f64, post- and pre-correction.
+GRIDDING_CASES = [
+    ((1, 16, 16, 16), None, "f32", True), ((1, 16, 16, 16), None, "f64", False),
+    ((2, 9, 12, 7), None, "f32", False), ((2, 9, 12, 7), None, "f64", True),
+    ((1, 1, 20, 21), None, "f32", True), ((1, 24, 1, 1), None, "f32", False),
+    ((3, 10, 8, 6), (1, 10, 8, 6), "f32", True),
+]
+
+
+def write_gridding(ref_gridding) -> int:
+    for k, (shape, in_shape, dt, post) in enumerate(GRIDDING_CASES):
+        rng = np.random.default_rng(500 + k)
+        typ = np.float32 if dt == "f32" else np.float64
+        inp = rng.standard_normal(in_shape or shape).astype(typ)
+        src = np.broadcast_to(inp, shape) if in_shape else inp
+        out = np.zeros(shape, dtype=typ)
+        status, err = ref_gridding(np.ascontiguousarray(src) if in_shape is None else src, out, post)
+        assert status == 0, err
+        meta = json.dumps({"func": "gridding", "shape": list(shape), "dtype": dt, "post": post,
+                           "broadcast": in_shape is not None})
+        np.savez_compressed(os.path.join(HERE, f"h{k:03d}_gridding.npz"), meta=np.array(meta), inp=inp, out=out)
+    return len(GRIDDING_CASES)
+
+
 def main() -> None:
     ref = RefLib()
     for f in os.listdir(HERE):
         if f.endswith(".npz"):
             os.remove(os.path.join(HERE, f))
+    print("wrote", write_gridding(ref_gridding_correction), "gridding fixtures")
     for k, c in enumerate(golden_cases()):
         call = build(c)
         out = clone(call)

@@ -14,7 +14,8 @@ import pytest
 from cases import build, case_id, clone, pin_cases, rel_l2
 from oracle.oracle import Call, FpOracle, RefLib, fp_available, ref_available
 
-GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "g*.npz")))
+GOLDEN_GRIDDING = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "h*_gridding.npz")))
 
 pytestmark = pytest.mark.skipif(not fp_available(), reason="oracle not built (make -C oracle fp)")
 
@@ -105,9 +106,43 @@ def test_known_answer_identity_extract():
 
 
 # ---------------------------------------------------------------------------------------------------
-# Gridding correction. The reference's GriddingCorrection does not compile (FourierProject.hpp:1034),
-# so the oracle is checked against an independent numpy restatement of its documented formula.
+# Gridding correction. As published, the reference's GriddingCorrection does not compile
+# (FourierProject.hpp:1034 hands Vec::from_vec the single bool of `l_shape != 1`); oracle/_ref builds it
+# with that expression written per element (oracle/ref_gridding.cpp), and the oracle is pinned bit for
+# bit to that build: to its fixtures (h*_gridding.npz) and, where it was built, to the library itself.
+# The numpy restatement of the documented formula below is an independent check.
 # ---------------------------------------------------------------------------------------------------
+@pytest.mark.parametrize("path", GOLDEN_GRIDDING, ids=[os.path.basename(p) for p in GOLDEN_GRIDDING])
+def test_oracle_gridding_matches_reference_golden(path):
+    from oracle.oracle import gridding_correction
+    z = np.load(path)
+    c = json.loads(str(z["meta"]))
+    shape = tuple(c["shape"])
+    inp = z["inp"]
+    src = np.broadcast_to(inp, shape) if c["broadcast"] else inp
+    out = np.zeros(shape, dtype=inp.dtype)
+    assert gridding_correction(src, out, post_correction=c["post"]) == 0
+    np.testing.assert_array_equal(out, z["out"])
+
+
+def test_gridding_fixtures_present():
+    assert len(GOLDEN_GRIDDING) >= 7
+
+
+@pytest.mark.skipif(not ref_available(), reason="reference CPU path not built (make -C oracle ref)")
+@pytest.mark.parametrize("shape", [(1, 32, 32, 32), (1, 33, 31, 17), (2, 5, 1, 40), (1, 64, 64, 1)])
+@pytest.mark.parametrize("post", [True, False])
+def test_oracle_gridding_matches_reference_library(shape, post):
+    from oracle.oracle import gridding_correction, ref_gridding_correction
+    rng = np.random.default_rng(sum(shape) + post)
+    for dt in (np.float32, np.float64):
+        inp = rng.standard_normal(shape).astype(dt)
+        a, b = np.zeros(shape, dt), np.zeros(shape, dt)
+        assert gridding_correction(inp, a, post_correction=post) == 0
+        status, err = ref_gridding_correction(inp, b, post_correction=post, threads=4)
+        assert status == 0, err
+        np.testing.assert_array_equal(a, b)
+
 def _numpy_gridding(inp, shape, post):
     b, d, h, w = shape
     half = np.array([s / 2 if s != 1 else 0.0 for s in (d, h, w)])
