@@ -6,6 +6,8 @@ Two CPU implementations of noa's Fourier central-slice path, both callable on nu
   FP64 oracle). Always buildable (``make -C oracle fp``).
 * ``ref`` — oracle/_ref/libnoa_ref.so, the reference's own CPU (OpenMP) path compiled from its sources
   (``make -C oracle ref``). Present only where it was built.
+* ``ref_cuda`` — oracle/_ref/libnoa_ref_cuda.so (``make -C oracle ref-cuda``): noa's CUDA backend and the
+  reference-side binding, to pass a noa GPU Texture through the binding (GPU tests only).
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may import this module.
 """
@@ -289,6 +291,33 @@ def ref_gridding_correction(inp: np.ndarray, out: np.ndarray, post_correction: b
     err = C.create_string_buffer(512)
     status = fn(C.byref(a_in), C.byref(a_out), C.c_int32(int(post_correction)), C.c_int(threads), err, C.c_int(512))
     return status, err.value.decode(errors="replace")
+
+
+REF_CUDA_LIB = os.path.join(HERE, "_ref", "libnoa_ref_cuda.so")
+
+
+def ref_texture_extract(volume: np.ndarray, rotations: np.ndarray, interp: int = 1) -> tuple:
+    """Through noa's own CUDA backend (oracle/_ref/libnoa_ref_cuda.so, GPU only): builds a noa
+    Texture<c32> of `volume` ((1, n, n, n/2+1) complex64, hc layout) and runs the reference-side binding's
+    extract<HC2H> with it and with the plain device array. Returns (from_texture, from_array)."""
+    lib = C.CDLL(REF_CUDA_LIB)
+    n = volume.shape[1]
+    count = rotations.shape[0]
+    vol = np.ascontiguousarray(volume, dtype=np.complex64)
+    rot = np.ascontiguousarray(pack_transforms(rotations.astype(np.float32)))
+    a = np.zeros((count, 1, n, n // 2 + 1), np.complex64)
+    b = np.zeros_like(a)
+    err = C.create_string_buffer(512)
+    status = lib.noaref_texture_extract(C.c_void_p(vol.ctypes.data), C.c_int64(n), C.c_void_p(rot.ctypes.data),
+                                        C.c_int64(count), C.c_int32(interp), C.c_void_p(a.ctypes.data),
+                                        C.c_void_p(b.ctypes.data), err, C.c_int(512))
+    if status != 0:
+        raise RuntimeError(err.value.decode(errors="replace"))
+    return a, b
+
+
+def ref_cuda_available() -> bool:
+    return os.path.exists(REF_CUDA_LIB)
 
 
 def fp_available() -> bool:
