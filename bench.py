@@ -316,11 +316,108 @@ def run_gpu(args) -> None:
             "gpu_launches": 4 * args.steps,
             "clocks": clocks.summary(),
         }
+        if not args.no_secondary and world == 1:
+            line["secondary"] = secondary(args)
         if not args.no_cpu_baseline and world == 1:   # the CPU baseline is taken at N = 1 only
             line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------------------------------
+# Secondary workloads of the default line, bounded to well under a minute: the small per-call case
+# (64^3), the batched uneven LANCZOS8 extraction against its per-call form in the same run, and the
+# 512^3 windowed-sinc insertion on a subset of its slices, gather against scatter.
+# ---------------------------------------------------------------------------------------------------
+def _events_ms(fn, reps: int, warmup: int = 3, flush=None) -> float:
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(reps):
+        if flush is not None:
+            flush()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b.record()
+        torch.cuda.synchronize()
+        ts.append(a.elapsed_time(b))
+    return statistics.median(ts)
+
+
+def secondary(args) -> dict:
+    import torch
+    from noa_b200 import fourier_project as fp
+    from noa_b200 import synthetic, workloads
+    t_start = time.perf_counter()
+    out = {}
+
+    # 64^3: extract 64 slices (hc2h) then rasterize 64 slices (h2hc, + weights), one call each.
+    n, b = 64, 64
+    vol = torch.from_numpy(synthetic.make_volume(n, seed=0)).cuda()
+    rot = fp.pack_rotations(torch.from_numpy(synthetic.random_rotations(b, seed=2)).cuda())
+    sl = torch.empty((b, 1, n, n // 2 + 1), dtype=torch.complex64, device="cuda")
+    grid = torch.zeros((1, n, n, n // 2 + 1), dtype=torch.complex64, device="cuda")
+    grid_w = torch.zeros((1, n, n, n // 2 + 1), dtype=torch.float32, device="cuda")
+    ext = _events_ms(lambda: fp.extract_central_slices_3d("hc2h", vol, None, (1, n, n, n), sl, None, (b, 1, n, n),
+                                                          None, rot), 50)
+    ras = _events_ms(lambda: fp.rasterize_central_slices_3d("h2hc", sl, None, (b, 1, n, n), grid, grid_w,
+                                                            (1, n, n, n), None, rot), 50)
+    out["per_call_64"] = {"workload": "extract 64 slices of 64x33 c64 (hc2h) from a 64^3 rfft volume; rasterize "
+                                      "them (h2hc) into 64^3 + f32 weights; LINEAR, cutoff 0.5",
+                          "extract_ms": ext, "rasterize_ms": ras,
+                          "slices_per_s": 2 * b / ((ext + ras) * 1e-3), "timing": "median of 50 calls, L2 warm"}
+    del vol, sl, grid, grid_w
+
+    # Batched uneven LANCZOS8: 12,000 extractions over 12 volumes of 128-384, graph vs per call.
+    wargs = argparse.Namespace(seed=0, total=12000, interp="lanczos8", no_autotune=False, steps=3, warmup=2)
+    r = workloads.batched(wargs)
+    out["batched_lanczos8_12000"] = {
+        "workload": "12,000 LANCZOS8 extractions (hc2h) over 12 volumes of 128, 192, 256, 384, lognormal slice "
+                    "counts; one graph-captured persistent launch vs one call per request, same run",
+        "batched_ms": r["batched"]["ms"], "per_call_ms": r["per_call"]["ms"],
+        "batched_slices_per_s": r["batched"]["value"], "speedup_batched_vs_per_call": r["speedup_batched_vs_per_call"],
+        "timing": "median of 3, L2 flushed before each"}
+    torch.cuda.empty_cache()
+
+    # 512^3 windowed-sinc insertion (half-width 6 voxels), gather vs scatter form, on 1000 of the slices.
+    n, k = 512, 1000
+    wp = n // 2 + 1
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(11)
+    slices = workloads._device_slices(k, n, gen, torch.device("cuda"), bfactor=150.0, centered=True)
+    rot = fp.pack_rotations(torch.from_numpy(synthetic.random_rotations(k, seed=16)).cuda())
+    ws = fp.WindowedSinc(-1.0, 6.0 / n)
+    grids = {}
+    times = {}
+    for name, fn in (("gather", fp.insert_central_slices_3d), ("scatter", fp.insert_central_slices_3d_scatter)):
+        v = torch.zeros((1, n, n, wp), dtype=torch.complex64, device="cuda")
+        w = torch.zeros((1, n, n, wp), dtype=torch.float32, device="cuda")
+
+        def call():
+            fn("hc2hc", slices, None, (k, 1, n, n), v, w, (1, n, n, n), None, rot, interp="linear",
+               windowed_sinc=ws, fftfreq_cutoff=0.5)
+
+        call()
+        torch.cuda.synchronize()
+        grids[name] = v.clone()
+        times[name] = _events_ms(call, 3, warmup=0)
+        del v, w
+    x, y = grids["scatter"].to(torch.complex128), grids["gather"].to(torch.complex128)
+    agree = (torch.linalg.vector_norm(x - y) / torch.linalg.vector_norm(y)).item()
+    del grids, x, y, slices
+    torch.cuda.empty_cache()
+    out["insert_512_subset"] = {
+        "workload": f"windowed-sinc insertion (half-width 6 voxels, LINEAR in-plane, hc2hc, + weights) of {k} of "
+                    f"the 20,000 slices of 512x257 c64 into a 512^3 rfft volume",
+        "gather_ms": times["gather"], "scatter_ms": times["scatter"],
+        "gather_slices_per_s": k / (times["gather"] * 1e-3), "scatter_slices_per_s": k / (times["scatter"] * 1e-3),
+        "scatter_vs_gather_rel_l2": agree, "timing": "median of 3 accumulating calls"}
+    out["seconds"] = time.perf_counter() - t_start
+    return out
 
 
 # ---------------------------------------------------------------------------------------------------
@@ -802,6 +899,9 @@ def main() -> None:
     p.add_argument("--e2e-steps", type=int, default=5)
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-secondary", action="store_true",
+                   help="skip the secondary workloads of the default line (64^3 per call, batched LANCZOS8, "
+                        "512^3 insertion subset)")
     p.add_argument("--ref-batch", type=int, default=None,
                    help="slices per CPU call of the reference arm (default: enough for noa to use every thread)")
     p.add_argument("--n", type=int, default=None, help="box size (default 256, or 512 for insert_512)")
