@@ -62,6 +62,8 @@ __device__ __forceinline__ void extract_rows_pairs(const ProjArgs& a, const floa
     const float f1 = div(static_cast<float>(u), a.f_slice1);
     float2 value[PAIRS_PPT];
     bool inside[PAIRS_PPT];
+    const float* m = nullptr;
+    const bool lean = lean_rotation(a, b, m);
 #pragma unroll
     for (int r = 0; r < PAIRS_PPT; ++r) {
         const int y = y0 + r * dy;
@@ -71,7 +73,10 @@ __device__ __forceinline__ void extract_rows_pairs(const ProjArgs& a, const floa
             continue;
         const float f0 = div(static_cast<float>(index2frequency(a.out_centered, y, a.slice_h)), a.f_slice0);
         float fz, fy, fx;
-        slice2grid(f0, f1, a.scale, a.rot, b, a.ews, fz, fy, fx);
+        if (lean)
+            slice2grid_lean(m, f0, f1, fz, fy, fx);
+        else
+            slice2grid(f0, f1, a.scale, a.rot, b, a.ews, fz, fy, fx);
         inside[r] = dot3(fz, fy, fx, fz, fy, fx) <= a.cutoff_sqd;
         if (inside[r])
             value[r] = to_output<true, OUT_C>(interp_linear_pairs(pairs, a.vol_h * WP, WP, sp, mul(fz, a.target0),

@@ -83,10 +83,15 @@ extract_pairs_kernel(const __grid_constant__ ProjArgs a, const float4* __restric
     for (int64_t b = blockIdx.y; b < a.n_slices; b += gridDim.y) {
         float2 value[PAIR_PPT];
         bool inside[PAIR_PPT];
+        const float* m = nullptr;
+        const bool lean = lean_rotation(a, b, m);
 #pragma unroll
         for (int r = 0; r < PAIR_PPT; ++r) {
             float fz, fy, fx;
-            slice2grid(f0[r], f1, a.scale, a.rot, b, a.ews, fz, fy, fx);
+            if (lean)
+                slice2grid_lean(m, f0[r], f1, fz, fy, fx);
+            else
+                slice2grid(f0[r], f1, a.scale, a.rot, b, a.ews, fz, fy, fx);
             value[r] = make_float2(0.f, 0.f);
             inside[r] = y0 + r * TY < a.slice_h && dot3(fz, fy, fx, fz, fy, fx) <= a.cutoff_sqd;
             if (inside[r])

@@ -29,6 +29,33 @@ __device__ __forceinline__ float2 interp_linear_pairs(const float4* __restrict__
     const bool okx0 = b2 >= 0 && b2 <= hi2;
     const bool okx1 = b2 + 1 >= 0 && b2 + 1 <= hi2;
     float2 value = make_float2(0.f, 0.f);
+    // Interior cells (every tap inside the volume, the two rows of each axis adjacent in memory: not
+    // across the non-centered layout's wrap at -1): the same terms in the same order, from one base
+    // offset, with the four loads issued together.
+    if (b0 >= lo0 && b0 + 1 <= hi0 && b1 >= lo1 && b1 + 1 <= hi1 && okx0 && okx1 &&
+        (sp.centered || (b0 != -1 && b1 != -1))) {
+        const float4* p = pairs + (frequency2index(sp.centered, b0, sp.n0) * sz +
+                                   frequency2index(sp.centered, b1, sp.n1) * sy + b2);
+        float4 q[4];
+        q[0] = ldg_evict_last_half(p);
+        q[1] = ldg_evict_last_half(p + sy);
+        q[2] = ldg_evict_last_half(p + sz);
+        q[3] = ldg_evict_last_half(p + sz + sy);
+#pragma unroll
+        for (int z = 0; z < 2; ++z) {
+            float2 vz = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int y = 0; y < 2; ++y) {
+                float2 vy = make_float2(0.f, 0.f);
+                vy = cfma(make_float2(q[z * 2 + y].x, q[z * 2 + y].y), w20, vy);
+                vy = cfma(make_float2(q[z * 2 + y].z, q[z * 2 + y].w), t2, vy);
+                vz = cfma(vy, w1[y], vz);
+            }
+            value = cfma(vz, w0[z], value);
+        }
+        value.y *= conjugate;
+        return value;
+    }
 #pragma unroll
     for (int z = 0; z < 2; ++z) {
         const int iz = b0 + z;
@@ -52,6 +79,24 @@ __device__ __forceinline__ float2 interp_linear_pairs(const float4* __restrict__
     }
     value.y *= conjugate;
     return value;
+}
+
+// slice2grid for a Mat33 rotation with no scaling and no Ewald curvature, when the slice's matrix
+// column 0 is finite: rotate() computes ((m_k0 * 0) + (m_k1 * f0)) + (m_k2 * f1), and for finite m_k0
+// the first product is a zero whose sign never reaches the result (the coordinates then decide the
+// cutoff, the cell, its weights and the Friedel flip the same way), so it is left out.
+__device__ __forceinline__ void slice2grid_lean(const float* m, float f0, float f1, float& z, float& y, float& x) {
+    z = add(mul(m[1], f0), mul(m[2], f1));
+    y = add(mul(m[4], f0), mul(m[5], f1));
+    x = add(mul(m[7], f0), mul(m[8], f1));
+}
+
+// Whether slice b of `a` can take slice2grid_lean; `m` is then its matrix.
+__device__ __forceinline__ bool lean_rotation(const ProjArgs& a, int64_t b, const float*& m) {
+    if (a.rot.kind != 2 || a.scale.kind != 0 || a.ews.on)
+        return false;
+    m = xform_ptr(a.rot, b, 12);
+    return isfinite(m[0]) && isfinite(m[3]) && isfinite(m[6]);
 }
 
 // Whether a call may read the pair copy: LINEAR, complex volume given as an array, no input weights,
