@@ -1,4 +1,5 @@
-/* noa_b200 — batched extraction: many extract_central_slices_3d calls in one persistent launch.
+/* noa_b200 — batched extraction (many extract_central_slices_3d calls in one persistent launch) and
+ * batched rasterization (many rasterize_central_slices_3d calls in one launch of each kernel).
  *
  * No single function of the reference corresponds to this: it executes a list of
  * extract_central_slices_3d calls (noa/xform/FourierProject.hpp:1869-1914) — different volumes, box
@@ -89,6 +90,31 @@ NB_API int nb_extract_batch_launch(int32_t remap, const nb_extract_request_ex* r
                                    const nb_options* options, void* stream);
 
 NB_API int nb_extract_batch_destroy(nb_extract_batch batch);
+
+/* ---- Batched rasterization (used by serving loops) ------------------------------------------------ */
+
+/* One rasterization: the arguments of nb_rasterize_central_slices_3d. */
+typedef struct {
+    const nb_array* slice;
+    const nb_array* slice_weight;      /* nullable */
+    int64_t slice_shape[4];
+    const nb_array* volume;
+    const nb_array* volume_weight;     /* nullable */
+    int64_t volume_shape[4];
+    const nb_transform* inv_scaling;   /* nullable */
+    const nb_transform* fwd_rotation;
+} nb_rasterize_request;
+
+/* No counterpart in the reference: a list of rasterize_central_slices_3d calls
+ * (FourierProject.hpp:1653-1692), each into its own grids, enqueued on `stream` as ONE scatter launch and
+ * ONE finalize launch instead of a launch sequence per call. Each request is validated like
+ * nb_rasterize_central_slices_3d and sums the same terms (the order of the atomic additions may differ,
+ * as between two per-call runs). All requests share `remap` and `options`, their value types and the
+ * presence of output weights; their output grids must not overlap (NB_ERROR_INVALID otherwise). The
+ * accumulators of all requests come from one stream-ordered allocation (NB_ERROR_OOM without it). The
+ * request structs may be freed on return; the device buffers must stay valid until the work completes. */
+NB_API int nb_rasterize_batch_launch(int32_t remap, const nb_rasterize_request* requests, int64_t n_requests,
+                                     const nb_options* options, void* stream);
 
 #ifdef __cplusplus
 }

@@ -1,4 +1,4 @@
-"""Batched extraction (Python side of include/noa_b200/batch.h).
+"""Batched extraction and rasterization (Python side of include/noa_b200/batch.h).
 
 ``ExtractBatch`` takes a list of extract_central_slices_3d calls — any mix of volumes, box sizes and
 slice counts — and runs them as one persistent kernel captured in a CUDA graph. Build it once, then
@@ -65,7 +65,59 @@ def _setup(lib):
     lib.nb_extract_batch_launch.argtypes = [C.c_int32, C.POINTER(NbExtractRequestEx), C.c_int64,
                                             C.POINTER(fp.NbOptions), C.c_void_p]
     lib.nb_extract_batch_launch.restype = C.c_int
+    lib.nb_rasterize_batch_launch.argtypes = [C.c_int32, C.POINTER(NbRasterizeRequest), C.c_int64,
+                                              C.POINTER(fp.NbOptions), C.c_void_p]
+    lib.nb_rasterize_batch_launch.restype = C.c_int
     lib._nb_batch_ready = True
+
+
+class NbRasterizeRequest(C.Structure):
+    _fields_ = [("slice", C.POINTER(fp.NbArray)), ("slice_weight", C.POINTER(fp.NbArray)),
+                ("slice_shape", C.c_int64 * 4), ("volume", C.POINTER(fp.NbArray)),
+                ("volume_weight", C.POINTER(fp.NbArray)), ("volume_shape", C.c_int64 * 4),
+                ("inv_scaling", C.POINTER(fp.NbTransform)), ("fwd_rotation", C.POINTER(fp.NbTransform))]
+
+
+@dataclass
+class RasterizeRequest:
+    """The arguments of one rasterize_central_slices_3d call (each request owns its output grids)."""
+    slice: object
+    slice_shape: tuple
+    volume: object
+    volume_shape: tuple
+    fwd_rotation: object
+    volume_weight: object = None
+    slice_weight: object = None
+    inv_scaling: object = None
+
+
+def rasterize_batch_launch(remap: str, requests: list[RasterizeRequest], *, fftfreq_cutoff=0.5,
+                           target_shape=None, ews_radius=(0.0, 0.0), stream=None) -> None:
+    """Enqueues many rasterize_central_slices_3d calls, each into its own grids, as one scatter launch
+    and one finalize launch on ``stream`` (nb_rasterize_batch_launch)."""
+    lib = fp.lib()
+    _setup(lib)
+    keep = []
+    reqs = (NbRasterizeRequest * len(requests))()
+    for i, r in enumerate(requests):
+        q = reqs[i]
+        arrays = [fp.as_nb_array(t, keep) for t in (r.slice, r.slice_weight, r.volume, r.volume_weight)]
+        keep.extend(a for a in arrays if a is not None)
+        q.slice = C.pointer(arrays[0])
+        q.slice_weight = C.pointer(arrays[1]) if arrays[1] is not None else None
+        q.volume = C.pointer(arrays[2])
+        q.volume_weight = C.pointer(arrays[3]) if arrays[3] is not None else None
+        for k in range(4):
+            q.slice_shape[k] = int(r.slice_shape[k])
+            q.volume_shape[k] = int(r.volume_shape[k])
+        sc = fp.as_nb_transform(r.inv_scaling, False, keep)
+        rot = fp.as_nb_transform(r.fwd_rotation, True, keep)
+        keep.extend([sc, rot])
+        q.inv_scaling = C.pointer(sc)
+        q.fwd_rotation = C.pointer(rot)
+    opts = fp._options(fftfreq_cutoff=fftfreq_cutoff, target_shape=target_shape, ews_radius=ews_radius)
+    fp._check(lib.nb_rasterize_batch_launch(fp.REMAPS[remap], reqs, len(requests), C.byref(opts),
+                                            fp._stream_ptr(stream)))
 
 
 def _fill_request(q: NbExtractRequest, r: ExtractRequest, keep: list) -> None:

@@ -264,20 +264,14 @@ __device__ __forceinline__ unsigned slide_mask(unsigned m, bool up, bool dn) {
     return m;
 }
 
+// One run: column u, rows [y0, y0 + RUN) of slice b, into the accumulator.
 template<bool IN_C, bool OUT_C, bool W>
-__global__ void __launch_bounds__(RASTER_THREADS, 3)
-rasterize_runs_kernel(const __grid_constant__ ProjArgs a, const AccGrid g, void* __restrict__ acc) {
-    const int wp = a.slice_w / 2 + 1;
-    const int t = blockIdx.x * RASTER_THREADS + threadIdx.x;
-    const int u = t % wp;
-    const int y0 = (t / wp) * RUN;
-    if (y0 >= a.slice_h)
-        return;
+__device__ __forceinline__ void rasterize_run(const ProjArgs& a, const AccGrid& g, void* __restrict__ acc,
+                                              int64_t b, int u, int y0) {
     const int y_end = min(y0 + RUN, a.slice_h);
     const bool has_in_w = a.in_w.present;
     const float f1 = div(static_cast<float>(u), a.f_slice1);
-
-    for (int64_t b = blockIdx.y; b < a.n_slices; b += gridDim.y) {
+    {
         float2 cv[8];
         float cw[8];
         unsigned mask = 0;
@@ -375,6 +369,19 @@ rasterize_runs_kernel(const __grid_constant__ ProjArgs a, const AccGrid g, void*
     }
 }
 
+template<bool IN_C, bool OUT_C, bool W>
+__global__ void __launch_bounds__(RASTER_THREADS, 3)
+rasterize_runs_kernel(const __grid_constant__ ProjArgs a, const AccGrid g, void* __restrict__ acc) {
+    const int wp = a.slice_w / 2 + 1;
+    const int t = blockIdx.x * RASTER_THREADS + threadIdx.x;
+    const int u = t % wp;
+    const int y0 = (t / wp) * RUN;
+    if (y0 >= a.slice_h)
+        return;
+    for (int64_t b = blockIdx.y; b < a.n_slices; b += gridDim.y)
+        rasterize_run<IN_C, OUT_C, W>(a, g, acc, b, u, y0);
+}
+
 template<bool OUT_C, bool W>
 __device__ __forceinline__ void acc_accumulate(const void* acc, int off, float2& v, float& w) {
     const typename AccElem<OUT_C, W>::T s = static_cast<const typename AccElem<OUT_C, W>::T*>(acc)[off];
@@ -388,15 +395,14 @@ __device__ __forceinline__ void acc_accumulate(const void* acc, int off, float2&
 // each voxel: frequency2index(f) == i. Centered: f = i - n/2 only. Non-centered: f = i and f = i - n
 // (frequency2index wraps negative frequencies, so a tap past the Nyquist frequency lands on the
 // opposite side, as in the reference).
+// Voxel i (linear index over D x H x W/2+1) of the caller's grids.
 template<bool OUT_C, bool W>
-__global__ void finalize_padded_kernel(const __grid_constant__ ProjArgs a, const AccGrid g,
-                                       const void* __restrict__ acc) {
+__device__ __forceinline__ void finalize_padded_voxel(const ProjArgs& a, const AccGrid& g,
+                                                      const void* __restrict__ acc, int64_t i) {
     const int D = a.vol_d, H = a.vol_h, WP = a.vol_w / 2 + 1;
     const bool vc = a.out_centered;
-    const int64_t n = static_cast<int64_t>(D) * H * WP;
     const int ny = 2 * g.r1 + 1;
-    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
-         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    {
         const int x = static_cast<int>(i % WP);
         const int64_t zy = i / WP;
         const int y = static_cast<int>(zy % H), z = static_cast<int>(zy / H);
@@ -422,6 +428,15 @@ __global__ void finalize_padded_kernel(const __grid_constant__ ProjArgs a, const
         if constexpr (W)
             store_real(a.out_w, z, y, x, add(load_real(a.out_w, z, y, x), w));
     }
+}
+
+template<bool OUT_C, bool W>
+__global__ void finalize_padded_kernel(const __grid_constant__ ProjArgs a, const AccGrid g,
+                                       const void* __restrict__ acc) {
+    const int64_t n = static_cast<int64_t>(a.vol_d) * a.vol_h * (a.vol_w / 2 + 1);
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        finalize_padded_voxel<OUT_C, W>(a, g, acc, i);
 }
 
 // grid += scratch values; weights += scratch weights (caller's strides).

@@ -185,3 +185,70 @@ def test_linear_batch_scaled_and_curved_match_per_call(tmp_path, monkeypatch):
         torch.cuda.synchronize()
         assert torch.equal(r.slice, ref)
     batch.close()
+
+
+# ---------------------------------------------------------------------------------------------------
+# Batched rasterization: each request of one launch equals its own per-call rasterization (the same
+# terms; the atomic summation order may differ) and the oracle within the rasterization bar.
+# ---------------------------------------------------------------------------------------------------
+def _raster_requests(out_dt="c32", weights=True, counts=((32, 10), (48, 3), (64, 25), (40, 7)), seed=30):
+    import torch
+    from noa_b200 import synthetic
+    from noa_b200.batch import RasterizeRequest
+    reqs = []
+    for i, (n, count) in enumerate(counts):
+        sl = synthetic.make_slices(count, n, seed=seed + i)
+        if out_dt == "f32":
+            sl = np.ascontiguousarray(sl.real)
+        rot = synthetic.random_rotations(count, seed=seed + 20 + i)
+        dt = torch.complex64 if out_dt == "c32" else torch.float32
+        reqs.append(RasterizeRequest(
+            slice=torch.from_numpy(sl).cuda(), slice_shape=(count, 1, n, n),
+            volume=torch.zeros((1, n, n, n // 2 + 1), dtype=dt, device="cuda"), volume_shape=(1, n, n, n),
+            volume_weight=torch.zeros((1, n, n, n // 2 + 1), dtype=torch.float32, device="cuda") if weights else None,
+            fwd_rotation=torch.from_numpy(rot).cuda()))
+    return reqs
+
+
+@pytest.mark.parametrize("out_dt,weights", [("c32", True), ("c32", False), ("f32", True)])
+def test_rasterize_batch_matches_per_call_and_oracle(out_dt, weights):
+    import torch
+    from noa_b200 import fourier_project as fp
+    from noa_b200.batch import rasterize_batch_launch
+    from oracle.oracle import Call, FpOracle
+    reqs = _raster_requests(out_dt, weights)
+    rasterize_batch_launch("h2hc", reqs)
+    torch.cuda.synchronize()
+    for r in reqs:
+        v = torch.zeros_like(r.volume)
+        w = torch.zeros_like(r.volume_weight) if weights else None
+        fp.rasterize_central_slices_3d("h2hc", r.slice, None, r.slice_shape, v, w, r.volume_shape, None,
+                                       r.fwd_rotation)
+        torch.cuda.synchronize()
+        assert rel_l2(r.volume.cpu().numpy(), v.cpu().numpy()) <= 1e-6
+        call = Call(func="rasterize", remap="h2hc", inp=r.slice.cpu().numpy(), in_shape=r.slice_shape,
+                    out=np.zeros(tuple(r.volume.shape), np.complex64 if out_dt == "c32" else np.float32),
+                    out_shape=r.volume_shape, rot=r.fwd_rotation.cpu().numpy(),
+                    out_w=np.zeros(tuple(r.volume.shape), np.float32) if weights else None)
+        FpOracle().run(call, 4)
+        assert rel_l2(r.volume.cpu().numpy(), call.out) <= 1e-4
+        if weights:
+            assert rel_l2(w.cpu().numpy(), r.volume_weight.cpu().numpy()) <= 1e-6
+            assert rel_l2(r.volume_weight.cpu().numpy(), call.out_w) <= 1e-4
+
+
+def test_rasterize_batch_rejects_shared_grids_and_mixed_types():
+    import torch
+    from noa_b200 import fourier_project as fp
+    from noa_b200.batch import rasterize_batch_launch
+    reqs = _raster_requests(counts=((32, 3), (32, 4)))
+    reqs[1].volume = reqs[0].volume  # both requests would add into the same grid
+    with pytest.raises(fp.NoaB200Error) as e:
+        rasterize_batch_launch("h2hc", reqs)
+    assert e.value.code == fp.NB_ERROR_INVALID and "disjoint" in str(e.value)
+    reqs = _raster_requests(counts=((32, 3), (32, 4)))
+    reqs[1].volume_weight = None
+    with pytest.raises(fp.NoaB200Error) as e:
+        rasterize_batch_launch("h2hc", reqs)
+    assert e.value.code == fp.NB_ERROR_INVALID
+    torch.cuda.synchronize()
