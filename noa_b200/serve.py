@@ -11,23 +11,25 @@ their slices). ``ProjectionServer.poll()`` runs one scheduling round:
 3. launches — admitted extractions are packed, up to ``max_batch_slices`` slices, into ONE persistent
    launch (``nb_extract_batch_launch``: a device work queue over all of them, each volume read through
    its resident pair copy) on the extraction stream, with at most ``max_inflight_batches`` batches
-   queued there; admitted insertions each get a rasterization into their own zeroed value + weight
-   accumulator on one of the insertion streams, round robin.
+   queued there; the insertions admitted in the round are packed the same way into ONE batched
+   rasterization (``nb_rasterize_batch_launch``: one scatter and one finalize launch, each request into
+   its own zeroed value + weight grids) on one of the insertion streams, round robin.
 
 Backpressure and cancellation: with ``max_waiting`` set, ``submit()`` refuses a request while that many
 wait for admission (it raises ``ServerBusy``; the client keeps the request and offers it again, as
 ``run_stream`` does), so the queue and the host memory it pins stay bounded under overload.
-``cancel()`` withdraws a request that has not been launched yet (waiting, or an admitted extraction
-not yet packed into a batch, whose memory returns to the budget); work already on the device cannot be
+``cancel()`` withdraws a request that has not been launched yet (waiting, or admitted but not yet
+packed into a launch, whose memory returns to the budget); work already on the device cannot be
 recalled, so such a request completes normally.
 
 Continuous batching: extractions that arrive while a batch runs are admitted as memory frees up and
 form the next batch, which is already queued behind the running one, so the device never waits for
-the host; insertions run concurrently on their own streams. The scheduling logic is independent of
+the host; insertion batches run concurrently on their own streams. The scheduling logic is independent of
 CUDA (``Executor``), so it is tested on the CPU with a simulated executor.
 
 No function of the reference corresponds to this module; it drives extract_central_slices_3d
-(FourierProject.hpp:1869-1914) and rasterize_central_slices_3d (:1653-1692) through this library.
+(FourierProject.hpp:1869-1914) and rasterize_central_slices_3d (:1653-1692) through this library's
+batched entry points.
 """
 from __future__ import annotations
 
@@ -110,7 +112,7 @@ class Executor:
     def launch_extracts(self, reqs: list[Request], vols: list[Volume]) -> Any:
         raise NotImplementedError
 
-    def launch_insert(self, req: Request, vol: Volume) -> Any:
+    def launch_inserts(self, reqs: list[Request], vols: list[Volume]) -> Any:
         raise NotImplementedError
 
     def done(self, token) -> bool:
@@ -208,22 +210,25 @@ class CudaExecutor(Executor):
         self.host_seconds += time.perf_counter() - h0
         return ev
 
-    def launch_insert(self, req, vol):
+    def launch_inserts(self, reqs, vols):
         torch = self.torch
         s = self.insert_streams[self._next % len(self.insert_streams)]
         self._next += 1
-        box = vol.box
         h0 = time.perf_counter()
         start = self._span_start(s)
+        calls = []
         with torch.cuda.stream(s):
-            values = torch.zeros((1, box, box, box // 2 + 1), dtype=torch.complex64, device=self.device)
-            weights = torch.zeros((1, box, box, box // 2 + 1), dtype=torch.float32, device=self.device)
-            req.output = (values, weights)
-            n = req.n_slices
-            self.fp.rasterize_central_slices_3d(self.remap_insert, req.slices, None, (n, 1, box, box), values,
-                                                weights, (1, box, box, box), None, self._rotations(req),
-                                                fftfreq_cutoff=self.cutoff, stream=s)
-        ev = self._span_end(start, s, "insert", req.n_slices)
+            for req, vol in zip(reqs, vols):
+                box = vol.box
+                values = torch.zeros((1, box, box, box // 2 + 1), dtype=torch.complex64, device=self.device)
+                weights = torch.zeros((1, box, box, box // 2 + 1), dtype=torch.float32, device=self.device)
+                req.output = (values, weights)
+                n = req.n_slices
+                calls.append(self.batch.RasterizeRequest(
+                    slice=req.slices, slice_shape=(n, 1, box, box), volume=values, volume_shape=(1, box, box, box),
+                    volume_weight=weights, fwd_rotation=self._rotations(req)))
+            self.batch.rasterize_batch_launch(self.remap_insert, calls, fftfreq_cutoff=self.cutoff, stream=s)
+        ev = self._span_end(start, s, "insert", sum(r.n_slices for r in reqs))
         self.host_seconds += time.perf_counter() - h0
         return ev
 
@@ -251,6 +256,7 @@ class ServerStats:
     batch_requests: int = 0
     batch_slices: int = 0
     inserts: int = 0
+    insert_batches: int = 0
     max_waiting: int = 0
     peak_bytes: int = 0
     poll_seconds: float = 0.0
@@ -279,6 +285,7 @@ class ProjectionServer:
         self.used = 0
         self.waiting: deque[Request] = deque()
         self.ready_extract: deque[Request] = deque()
+        self.ready_insert: deque[Request] = deque()
         self.inflight: list[tuple[Any, list[Request], bool]] = []  # (token, requests, is_batch)
         self.stats = ServerStats()
         self._rid = 0
@@ -331,7 +338,7 @@ class ProjectionServer:
         admitted extraction not yet in a batch, the launch queue (its memory returns to the budget).
         Returns True then, with ``req.error == "cancelled"``. Returns False for a request already on the
         device (it completes normally: its work cannot be recalled from the GPU), finished, or unknown."""
-        for queue, admitted in ((self.waiting, False), (self.ready_extract, True)):
+        for queue, admitted in ((self.waiting, False), (self.ready_extract, True), (self.ready_insert, True)):
             for i, r in enumerate(queue):
                 if r is req:
                     del queue[i]
@@ -345,7 +352,7 @@ class ProjectionServer:
         return False
 
     def busy(self) -> bool:
-        return bool(self.waiting or self.ready_extract or self.inflight)
+        return bool(self.waiting or self.ready_extract or self.ready_insert or self.inflight)
 
     def poll(self) -> list[Request]:
         """One scheduling round; returns the requests completed (or rejected) in it."""
@@ -401,16 +408,24 @@ class ProjectionServer:
             self.used += need
             self.stats.peak_bytes = max(self.stats.peak_bytes, self.resident + self.used)
             r.admitted = self.clock()
-            if r.kind == "extract":
-                self.ready_extract.append(r)
-            else:
-                r.launched = r.admitted
-                token = self.ex.launch_insert(r, self.volumes[r.volume_id])
-                self.inflight.append((token, [r], False))
-                self.stats.inserts += 1
+            (self.ready_extract if r.kind == "extract" else self.ready_insert).append(r)
         return rejected
 
     def _launch(self) -> None:
+        # Insertions admitted in this round: one batched rasterization, on the next insertion stream.
+        while self.ready_insert:
+            batch, slices = [], 0
+            while self.ready_insert and (not batch or slices + self.ready_insert[0].n_slices <= self.max_batch_slices):
+                r = self.ready_insert.popleft()
+                batch.append(r)
+                slices += r.n_slices
+            now = self.clock()
+            for r in batch:
+                r.launched = now
+            token = self.ex.launch_inserts(batch, [self.volumes[r.volume_id] for r in batch])
+            self.inflight.append((token, batch, False))
+            self.stats.inserts += len(batch)
+            self.stats.insert_batches += 1
         while self.ready_extract:
             n_batches = sum(1 for _, _, b in self.inflight if b)
             if n_batches >= self.max_inflight_batches:

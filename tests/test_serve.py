@@ -47,12 +47,13 @@ class FakeExecutor(Executor):
             r.output = ("slices", r.rid)
         return self._enqueue("extract", sum(r.n_slices for r in reqs))
 
-    def launch_insert(self, req, vol):
+    def launch_inserts(self, reqs, vols):
         q = f"insert{self._next % self.n_insert_queues}"
         self._next += 1
-        self.launches.append((q, [req.rid]))
-        req.output = ("grid", req.rid)
-        return self._enqueue(q, req.n_slices)
+        self.launches.append((q, [r.rid for r in reqs]))
+        for r in reqs:
+            r.output = ("grid", r.rid)
+        return self._enqueue(q, sum(r.n_slices for r in reqs))
 
     def done(self, token):
         return self.clock() >= token
@@ -151,17 +152,20 @@ def test_request_larger_than_the_budget_is_rejected_not_blocking():
     assert s.stats.rejected == 1
 
 
-def test_insertions_run_on_their_own_queues_concurrently():
+def test_insertions_of_a_round_form_one_batch_on_their_own_queue():
     s, ex, clock = make_server(10 ** 9)
     a = s.submit(Request("insert", 0, rot(100)))
     b = s.submit(Request("insert", 1, rot(100)))
     c = s.submit(Request("extract", 0, rot(100)))
     s.poll()
-    queues = [l[0] for l in ex.launches]
-    assert queues == ["insert0", "insert1", "extract"]
-    clock.t = 0.1
+    assert ex.launches == [("insert0", [a.rid, b.rid]), ("extract", [c.rid])]
+    d = s.submit(Request("insert", 1, rot(50)))
+    s.poll()
+    assert ex.launches[-1] == ("insert1", [d.rid])  # the next round's insertions take the next queue
+    assert s.stats.inserts == 3 and s.stats.insert_batches == 2
+    clock.t = 0.25
     done = s.poll()
-    assert {r.rid for r in done} == {a.rid, b.rid, c.rid}
+    assert {r.rid for r in done} == {a.rid, b.rid, c.rid, d.rid}
 
 
 def test_outputs_dropped_when_not_kept():
