@@ -425,8 +425,8 @@ __device__ __forceinline__ float2 interp_spectrum_2d(const SrcView& src, const S
         interp_weights<I>(sub(f0, fl0), w0);
         interp_weights<I>(sub(f1, fl1), w1);
         float2 value = make_float2(0.f, 0.f);
-        if constexpr (SIZE > 2) {
-            // Interior fast path (all taps in bounds, none flipped): same terms, same order.
+        {
+            // Interior fast path (all taps in bounds, none flipped per tap): same terms, same order.
             constexpr int END = SIZE / 2;
             if (b0 + START >= lo0 && b0 + END <= hi0 && b1 + START >= 0 && b1 + END <= hi1) {
 #pragma unroll
@@ -438,6 +438,8 @@ __device__ __forceinline__ float2 interp_spectrum_2d(const SrcView& src, const S
                         vy = cfma(read(iy, b1 + START + x), w1[x], vy);
                     value = cfma(vy, w0[y], value);
                 }
+                if (FLIP_EARLY)
+                    value.y *= conjugate;
                 return value;
             }
         }

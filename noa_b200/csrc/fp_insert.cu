@@ -23,6 +23,12 @@ insert_kernel(const __grid_constant__ ProjArgs a, int nbz, int nby, int nbx) {
     __shared__ int s_list[INSERT_THREADS];
     __shared__ int s_warp_count[INSERT_THREADS / 32];
     __shared__ int s_count;
+    // With a Mat33 rotation and neither scaling nor Ewald curvature, the kept slices' matrices are
+    // staged here (in list order) so that the voxel loop reads them from shared memory, computes the
+    // distance to the plane (row 0) first and the in-plane coordinates (rows 1 and 2) only inside the
+    // window: the same products and sums as grid2slice, in the same order.
+    __shared__ float s_mat[9][INSERT_THREADS];
+    const bool lean = a.rot.kind == 2 && a.scale.kind == 0 && !a.ews.on;
 
     const int D = a.vol_d, H = a.vol_h, WP = a.vol_w / 2 + 1;
     const bool vc = a.out_centered;
@@ -104,8 +110,16 @@ insert_kernel(const __grid_constant__ ProjArgs a, int nbz, int nby, int nbx) {
             int base = 0;
             for (int w = 0; w < warp; ++w)
                 base += s_warp_count[w];
-            if (keep)
-                s_list[base + __popc(ballot & ((1u << lane) - 1u))] = static_cast<int>(i - chunk);
+            if (keep) {
+                const int slot = base + __popc(ballot & ((1u << lane) - 1u));
+                s_list[slot] = static_cast<int>(i - chunk);
+                if (lean) {
+                    const float* m = xform_ptr(a.rot, i, 12);
+#pragma unroll
+                    for (int e = 0; e < 9; ++e)
+                        s_mat[e][slot] = m[e];
+                }
+            }
             if (tid == INSERT_THREADS - 1)
                 s_count = base + __popc(ballot);
             __syncthreads();
@@ -114,8 +128,16 @@ insert_kernel(const __grid_constant__ ProjArgs a, int nbz, int nby, int nbx) {
             if (active) {
                 for (int k = 0; k < count; ++k) {
                     const int64_t si = chunk + s_list[k];
-                    float f0, f1;
-                    const float zz = grid2slice(fz, fy, fx, a.scale, a.rot, si, a.ews, f0, f1);
+                    float f0, f1, zz;
+                    if (lean) {
+                        zz = dot3(s_mat[0][k], s_mat[1][k], s_mat[2][k], fz, fy, fx);
+                        if (!(fabsf(zz) <= a.fb))
+                            continue;
+                        f0 = dot3(s_mat[3][k], s_mat[4][k], s_mat[5][k], fz, fy, fx);
+                        f1 = dot3(s_mat[6][k], s_mat[7][k], s_mat[8][k], fz, fy, fx);
+                    } else {
+                        zz = grid2slice(fz, fy, fx, a.scale, a.rot, si, a.ews, f0, f1);
+                    }
                     if (fabsf(zz) <= a.fb) {
                         const float window = windowed_sinc_fast<true>(zz, a.pfs, a.ifs, a.pfb);
                         const float q0 = mul(f0, a.f_slice0), q1 = mul(f1, a.f_slice1);
