@@ -59,6 +59,7 @@ insert_extract_kernel(const __grid_constant__ ProjArgs a, int ntx, int tiles_per
     const bool has_out_w = a.out_w.present;
     const bool has_in_w = a.in_w.present;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const bool lean = a.rot.kind == 2 && a.scale.kind == 0 && !a.ews.on;
 
     for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
         const int64_t b = tile / tiles_per_slice;
@@ -157,8 +158,19 @@ insert_extract_kernel(const __grid_constant__ ProjArgs a, int ntx, int tiles_per
                             if (!in_cut)
                                 continue;
                             const int64_t si = super + list[g + j];
-                            float f0, f1;
-                            const float fz = grid2slice(sz, gy, gx, a.scale, a.rot, si, a.ews, f0, f1);
+                            float f0, f1, fz;
+                            if (lean) {
+                                // grid2slice's Mat33 rows, the distance to the plane first: the in-plane
+                                // rows are only needed inside the window (same products and sums).
+                                const float* m = xform_ptr(a.rot, si, 12);
+                                fz = dot3(m[0], m[1], m[2], sz, gy, gx);
+                                if (!(fabsf(fz) < a.fb))
+                                    continue;
+                                f0 = dot3(m[3], m[4], m[5], sz, gy, gx);
+                                f1 = dot3(m[6], m[7], m[8], sz, gy, gx);
+                            } else {
+                                fz = grid2slice(sz, gy, gx, a.scale, a.rot, si, a.ews, f0, f1);
+                            }
                             if (fabsf(fz) < a.fb) {
                                 const float ws = windowed_sinc_fast<true>(fz, a.pfs, a.ifs, a.pfb);
                                 const float q0 = mul(f0, a.f_in0), q1 = mul(f1, a.f_in1);
