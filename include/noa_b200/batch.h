@@ -42,9 +42,11 @@ typedef struct {
     double tuned_ms;       /* time of the chosen configuration while autotuning, or -1 */
     int32_t from_cache;    /* 1 if the configuration came from the autotune cache */
     int32_t min_ctas;      /* CTAs per SM the kernel variant was compiled for (its register cap) */
+    int32_t n_direct;      /* requests run as grids of their own (see nb_extract_batch_create) */
 } nb_batch_info;
 
-enum { NB_BATCH_AUTOTUNE = 1 };
+/* NB_BATCH_PERSISTENT_ONLY: every request goes through the persistent kernel (no direct grids). */
+enum { NB_BATCH_AUTOTUNE = 1, NB_BATCH_PERSISTENT_ONLY = 2 };
 
 /* Validates the requests, uploads their descriptors, chooses the launch configuration (with
  * NB_BATCH_AUTOTUNE: by timing the candidates on this batch, once per workload key, cached in memory and
@@ -53,7 +55,11 @@ enum { NB_BATCH_AUTOTUNE = 1 };
  * LINEAR batches over complex volumes (no scaling, EWS, input weights or w-window) hold a pair copy
  * (16 bytes per rfft voxel) of each volume whose requests read at least twice as many pixels as it
  * has voxels, like the per-call entry point; the graph rebuilds these copies at every run, so changes
- * to the volumes between runs are seen. */
+ * to the volumes between runs are seen. A request read through a pair copy with at least 2^23 output
+ * pixels runs, in the graph, as a grid of its own (the per-call pair kernel) on a parallel branch that
+ * starts when its volume's copy is written; the copies of the other volumes are made meanwhile on a
+ * higher-priority branch (NB_BATCH_PERSISTENT_ONLY keeps every request in the persistent kernel).
+ * Results are bit-identical either way. */
 NB_API int nb_extract_batch_create(int32_t remap, const nb_extract_request* requests, int64_t n_requests,
                                    const nb_options* options, int32_t flags, void* stream,
                                    nb_extract_batch* batch);
@@ -81,13 +87,19 @@ typedef struct {
     int64_t volume_pairs_bytes;
 } nb_extract_request_ex;
 
-/* Validates the requests and enqueues them on `stream` as ONE persistent launch (no graph, no
- * autotuning: the configuration cached for the workload key is used when there is one, else a default),
- * staging the descriptors in stream-ordered device memory. The request structs may be freed on return;
- * the device buffers must stay valid until the launch completes. Results are bit-identical to
- * nb_extract_central_slices_3d on each request. */
+/* Validates the requests and enqueues them on `stream` (no graph, no autotuning: the configuration
+ * cached for the workload key is used when there is one, else a default): each request read through
+ * its pair copy with at least 2^21 output pixels as a grid of its own (the per-call pair kernel), the
+ * others as ONE persistent launch, its descriptors staged in stream-ordered device memory. The request
+ * structs may be freed on return; the device buffers must stay valid until the launches complete.
+ * Results are bit-identical to nb_extract_central_slices_3d on each request. */
 NB_API int nb_extract_batch_launch(int32_t remap, const nb_extract_request_ex* requests, int64_t n_requests,
                                    const nb_options* options, void* stream);
+
+/* nb_extract_batch_launch with flags: NB_BATCH_PERSISTENT_ONLY sends every request through the
+ * persistent launch. */
+NB_API int nb_extract_batch_launch_ex(int32_t remap, const nb_extract_request_ex* requests, int64_t n_requests,
+                                      const nb_options* options, int32_t flags, void* stream);
 
 NB_API int nb_extract_batch_destroy(nb_extract_batch batch);
 

@@ -26,10 +26,11 @@ class NbExtractRequestEx(C.Structure):
 class NbBatchInfo(C.Structure):
     _fields_ = [("n_requests", C.c_int64), ("n_items", C.c_int64), ("tile_h", C.c_int32), ("tile_w", C.c_int32),
                 ("blocks_per_sm", C.c_int32), ("grid", C.c_int32), ("tuned_ms", C.c_double),
-                ("from_cache", C.c_int32), ("min_ctas", C.c_int32)]
+                ("from_cache", C.c_int32), ("min_ctas", C.c_int32), ("n_direct", C.c_int32)]
 
 
 NB_BATCH_AUTOTUNE = 1
+NB_BATCH_PERSISTENT_ONLY = 2
 
 
 @dataclass
@@ -65,6 +66,9 @@ def _setup(lib):
     lib.nb_extract_batch_launch.argtypes = [C.c_int32, C.POINTER(NbExtractRequestEx), C.c_int64,
                                             C.POINTER(fp.NbOptions), C.c_void_p]
     lib.nb_extract_batch_launch.restype = C.c_int
+    lib.nb_extract_batch_launch_ex.argtypes = [C.c_int32, C.POINTER(NbExtractRequestEx), C.c_int64,
+                                               C.POINTER(fp.NbOptions), C.c_int32, C.c_void_p]
+    lib.nb_extract_batch_launch_ex.restype = C.c_int
     lib.nb_rasterize_batch_launch.argtypes = [C.c_int32, C.POINTER(NbRasterizeRequest), C.c_int64,
                                               C.POINTER(fp.NbOptions), C.c_void_p]
     lib.nb_rasterize_batch_launch.restype = C.c_int
@@ -156,9 +160,11 @@ def volume_pairs(volume, volume_shape, stream=None):
 
 def extract_batch_launch(remap: str, requests: list[ExtractRequest], pairs: list | None = None, *,
                          interp="linear", fftfreq_cutoff=0.5, w_windowed_sinc=None, ews_radius=(0.0, 0.0),
-                         stream=None) -> None:
-    """Enqueues many extract_central_slices_3d calls as ONE persistent launch on ``stream`` (no graph,
-    no autotuning). ``pairs[i]`` is an optional ``volume_pairs`` copy of request i's volume."""
+                         persistent_only=False, stream=None) -> None:
+    """Enqueues many extract_central_slices_3d calls on ``stream`` (no graph, no autotuning): requests
+    of at least 2^21 output pixels read through their pair copy as grids of their own, the others as
+    ONE persistent launch (every request, with ``persistent_only``). ``pairs[i]`` is an optional
+    ``volume_pairs`` copy of request i's volume."""
     lib = fp.lib()
     _setup(lib)
     keep = []
@@ -171,16 +177,19 @@ def extract_batch_launch(remap: str, requests: list[ExtractRequest], pairs: list
             reqs[i].volume_pairs_bytes = p.numel() * p.element_size()
     opts = fp._options(interp=interp, fftfreq_cutoff=fftfreq_cutoff, ews_radius=ews_radius,
                        w_windowed_sinc=w_windowed_sinc)
-    fp._check(lib.nb_extract_batch_launch(fp.REMAPS[remap], reqs, len(requests), C.byref(opts),
-                                          fp._stream_ptr(stream)))
+    fp._check(lib.nb_extract_batch_launch_ex(fp.REMAPS[remap], reqs, len(requests), C.byref(opts),
+                                             NB_BATCH_PERSISTENT_ONLY if persistent_only else 0,
+                                             fp._stream_ptr(stream)))
 
 
 class ExtractBatch:
     """A captured batch of extractions. ``autotune=True`` times tile shapes and CTAs per SM on this
-    batch (once per workload key; the choice is cached) before capturing the launch."""
+    batch (once per workload key; the choice is cached) before capturing the launch. LINEAR requests
+    of at least 2^23 output pixels read through a pair copy run as grids of their own inside the
+    graph, unless ``persistent_only=True``."""
 
     def __init__(self, remap: str, requests: list[ExtractRequest], *, interp="linear", fftfreq_cutoff=0.5,
-                 w_windowed_sinc=None, ews_radius=(0.0, 0.0), autotune=True, stream=None):
+                 w_windowed_sinc=None, ews_radius=(0.0, 0.0), autotune=True, persistent_only=False, stream=None):
         lib = fp.lib()
         _setup(lib)
         self._lib = lib
@@ -194,7 +203,8 @@ class ExtractBatch:
                            w_windowed_sinc=w_windowed_sinc)
         handle = C.c_void_p()
         code = lib.nb_extract_batch_create(fp.REMAPS[remap], reqs, len(requests), C.byref(opts),
-                                           NB_BATCH_AUTOTUNE if autotune else 0, fp._stream_ptr(stream),
+                                           (NB_BATCH_AUTOTUNE if autotune else 0) |
+                                           (NB_BATCH_PERSISTENT_ONLY if persistent_only else 0), fp._stream_ptr(stream),
                                            C.byref(handle))
         fp._check(code)
         self._handle = handle
@@ -207,7 +217,7 @@ class ExtractBatch:
         fp._check(self._lib.nb_extract_batch_info(self._handle, C.byref(i)))
         return {"n_requests": i.n_requests, "n_items": i.n_items, "tile": (i.tile_h, i.tile_w),
                 "blocks_per_sm": i.blocks_per_sm, "grid": i.grid, "tuned_ms": i.tuned_ms,
-                "from_cache": bool(i.from_cache), "min_ctas": i.min_ctas}
+                "from_cache": bool(i.from_cache), "min_ctas": i.min_ctas, "n_direct": i.n_direct}
 
     def close(self) -> None:
         if getattr(self, "_handle", None):

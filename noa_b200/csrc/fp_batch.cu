@@ -51,6 +51,16 @@ struct BatchReq {
 static_assert(sizeof(BatchReq) % 8 == 0, "BatchReq is staged in shared memory as 8-byte words");
 
 constexpr int PAIRS_PPT = 4;
+// Output pixels from which a request over a pair copy gets a grid of its own (about 8 slices of 128^2;
+// smaller requests go through the persistent kernel). Measured on 12,000 LINEAR slices over 12
+// volumes of 128-384 as 12, 120 and 600 requests: with grids of their own on 4 branches, 4.76, 4.61
+// and 4.70 ms against 5.36, 5.78 and 6.57 ms all in the persistent kernel (per-call 4.94, 7.57, 13.2).
+constexpr int64_t DIRECT_MIN_PIXELS = int64_t(1) << 16;
+constexpr int N_SIDE = 4;  // graph branches the direct grids alternate on
+// The same for the one-shot launch, whose grids are launched one by one from the host (a few
+// microseconds each): 600 requests of ~20 slices as 596 grids took 16.9 ms against 6.6 ms in the
+// persistent kernel, so only requests worth ~20 us of device time or more get a grid there.
+constexpr int64_t ONESHOT_DIRECT_MIN_PIXELS = int64_t(1) << 21;
 
 // PAIRS_PPT output pixels (rows y0, y0 + dy, ...) of column u read through the volume's pair copy:
 // the body of extract_pairs_kernel (fp_extract.cu).
@@ -431,6 +441,19 @@ struct nb_extract_batch_t {
     // (their make_pairs launches are part of the graph), so later changes to the volumes are seen.
     std::vector<std::pair<nb::ProjArgs, float4*>> pair_jobs;
     bool pairs_only = false;  // every request reads a pair copy: the pairs-only kernel
+    // Requests over a pair copy with at least DIRECT_MIN_PIXELS output pixels leave the persistent
+    // kernel: each runs the per-call pair kernel as a grid of its own on one of N_SIDE branches of the
+    // graph, as soon as its volume's copy is written, while the copies of the next volumes are made on
+    // a higher-priority branch. The per-call kernel's per-pixel cost is lower than the persistent
+    // kernel's (no claims, request lookups or per-item tile setup), and with several branches the
+    // grids' ramps and tails overlap. (The copies, HBM-bound, overlap the extractions only a little:
+    // 0.62 ms of copies for 12 volumes of 128-384 saved 0.08 ms against copying first.)
+    std::vector<BatchReq> direct;
+    std::vector<size_t> direct_job;      // pair_jobs index of each direct request's copy
+    int64_t n_requests = 0;              // persistent + direct
+    cudaStream_t copy_stream = nullptr, side[N_SIDE] = {};
+    cudaEvent_t ev_fork = nullptr, ev_join[N_SIDE + 1] = {};
+    std::vector<cudaEvent_t> ev_pairs;   // one per pair job
 };
 
 namespace nb {
@@ -504,21 +527,66 @@ bool use_param(const nb_extract_batch_t* h) {
     return h->pairs_only && h->host_reqs.size() <= static_cast<size_t>(PACK);
 }
 
-cudaError_t launch(nb_extract_batch_t* h, const Config& c, cudaStream_t stream) {
+// The counter reset and the persistent kernel over the requests left in host_reqs.
+cudaError_t launch_persistent(nb_extract_batch_t* h, const Config& c, cudaStream_t stream) {
+    if (h->n_items == 0)
+        return cudaSuccess;
     const KernelFn fn = h->pairs_only ? pairs_only_kernel(h->out_cplx)
                                       : pick_kernel(h->interp, h->in_cplx, h->out_cplx, c.variant);
     const int grid = sm_count() * c.blocks_per_sm;
-    cudaError_t err = cudaSuccess;
-    for (const auto& job : h->pair_jobs)
-        if ((err = launch_make_pairs(job.first, job.second, stream)) != cudaSuccess)
-            return err;
-    err = cudaMemsetAsync(h->d_counter, 0, sizeof(unsigned long long), stream);
+    const cudaError_t err = cudaMemsetAsync(h->d_counter, 0, sizeof(unsigned long long), stream);
     if (err != cudaSuccess)
         return err;
     if (use_param(h))
         return launch_param(h->host_reqs, h->n_items, h->out_cplx, c.blocks_per_sm, h->d_counter, stream);
     fn<<<grid, 256, 0, stream>>>(h->d_reqs, static_cast<int>(h->host_reqs.size()), h->n_items, h->d_counter);
     return cudaGetLastError();
+}
+
+cudaError_t launch(nb_extract_batch_t* h, const Config& c, cudaStream_t stream) {
+    cudaError_t err = cudaSuccess;
+    if (h->direct.empty()) {
+        for (const auto& job : h->pair_jobs)
+            if ((err = launch_make_pairs(job.first, job.second, stream)) != cudaSuccess)
+                return err;
+        return launch_persistent(h, c, stream);
+    }
+    // Fork: copies on copy_stream, direct grids in turn on the side streams, the persistent kernel
+    // after the last copy on copy_stream; everything joins back into `stream`.
+    if ((err = cudaEventRecord(h->ev_fork, stream)) != cudaSuccess)
+        return err;
+    cudaStream_t branch[N_SIDE + 1] = {h->copy_stream};
+    for (int k = 0; k < N_SIDE; ++k)
+        branch[k + 1] = h->side[k];
+    for (cudaStream_t b : branch)
+        if ((err = cudaStreamWaitEvent(b, h->ev_fork, 0)) != cudaSuccess)
+            return err;
+    int least = 0, greatest = 0;
+    if ((err = cudaDeviceGetStreamPriorityRange(&least, &greatest)) != cudaSuccess)
+        return err;
+    for (size_t j = 0; j < h->pair_jobs.size(); ++j) {
+        if ((err = launch_make_pairs(h->pair_jobs[j].first, h->pair_jobs[j].second, h->copy_stream, &greatest)) !=
+            cudaSuccess)
+            return err;
+        if ((err = cudaEventRecord(h->ev_pairs[j], h->copy_stream)) != cudaSuccess)
+            return err;
+    }
+    for (size_t k = 0; k < h->direct.size(); ++k) {
+        const cudaStream_t s = h->side[k % N_SIDE];
+        if ((err = cudaStreamWaitEvent(s, h->ev_pairs[h->direct_job[k]], 0)) != cudaSuccess)
+            return err;
+        if ((err = launch_extract_pairs(h->direct[k].a, h->direct[k].pairs, s)) != cudaSuccess)
+            return err;
+    }
+    if ((err = launch_persistent(h, c, h->copy_stream)) != cudaSuccess)
+        return err;
+    for (int k = 0; k < N_SIDE + 1; ++k) {
+        if ((err = cudaEventRecord(h->ev_join[k], branch[k])) != cudaSuccess)
+            return err;
+        if ((err = cudaStreamWaitEvent(stream, h->ev_join[k], 0)) != cudaSuccess)
+            return err;
+    }
+    return cudaSuccess;
 }
 
 // Median of `reps` timed launches (after one warm-up), in milliseconds.
@@ -554,7 +622,7 @@ double time_config(nb_extract_batch_t* h, const Config& c, cudaStream_t stream, 
 // LINEAR over complex volumes: a pair copy per distinct volume whose requests read at least twice
 // as many pixels as it has voxels (the per-call rule), allocated for the batch's lifetime. Without
 // memory for a copy, its requests take the generic path.
-void plan_pairs(nb_extract_batch_t* h) {
+void plan_pairs(nb_extract_batch_t* h, bool allow_direct) {
     if (h->interp != I_LINEAR || !h->in_cplx)
         return;
     struct Vol { const ProjArgs* a; int64_t pixels; std::vector<size_t> reqs; };
@@ -587,10 +655,49 @@ void plan_pairs(nb_extract_batch_t* h) {
         for (size_t i : v.reqs)
             h->host_reqs[i].pairs = buf;
     }
-    bool all = !h->host_reqs.empty();
+    // Copies in increasing size, so the first direct grids start early and the largest copies overlap
+    // the extractions.
+    std::stable_sort(h->pair_jobs.begin(), h->pair_jobs.end(), [](const auto& x, const auto& y) {
+        return static_cast<int64_t>(x.first.vol_d) * x.first.vol_h * x.first.vol_w <
+               static_cast<int64_t>(y.first.vol_d) * y.first.vol_h * y.first.vol_w;
+    });
+    std::vector<BatchReq> keep;
+    for (size_t j = 0; j < h->pair_jobs.size(); ++j)
+        for (const BatchReq& r : h->host_reqs)
+            if (allow_direct && r.pairs == h->pair_jobs[j].second &&
+                r.a.n_slices * r.a.slice_h * static_cast<int64_t>(r.a.slice_w / 2 + 1) >= DIRECT_MIN_PIXELS) {
+                h->direct.push_back(r);
+                h->direct_job.push_back(j);
+            }
+    for (const BatchReq& r : h->host_reqs)
+        if (!(allow_direct && r.pairs &&
+              r.a.n_slices * r.a.slice_h * static_cast<int64_t>(r.a.slice_w / 2 + 1) >= DIRECT_MIN_PIXELS))
+            keep.push_back(r);
+    h->host_reqs.swap(keep);
+    bool all = true;
     for (const BatchReq& r : h->host_reqs)
         all = all && r.pairs != nullptr;
     h->pairs_only = all;
+}
+
+// Streams and events of a batch with direct requests (see nb_extract_batch_t::direct).
+cudaError_t make_branches(nb_extract_batch_t* h) {
+    if (h->direct.empty())
+        return cudaSuccess;
+    int least = 0, greatest = 0;
+    cudaError_t err = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    if (err == cudaSuccess)
+        err = cudaStreamCreateWithPriority(&h->copy_stream, cudaStreamNonBlocking, greatest);
+    for (int k = 0; k < N_SIDE && err == cudaSuccess; ++k)
+        err = cudaStreamCreateWithPriority(&h->side[k], cudaStreamNonBlocking, least);
+    if (err == cudaSuccess)
+        err = cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming);
+    for (int k = 0; k < N_SIDE + 1 && err == cudaSuccess; ++k)
+        err = cudaEventCreateWithFlags(&h->ev_join[k], cudaEventDisableTiming);
+    h->ev_pairs.assign(h->pair_jobs.size(), nullptr);
+    for (size_t j = 0; j < h->ev_pairs.size() && err == cudaSuccess; ++j)
+        err = cudaEventCreateWithFlags(&h->ev_pairs[j], cudaEventDisableTiming);
+    return err;
 }
 
 std::string workload_key(const nb_extract_batch_t* h) {
@@ -620,6 +727,14 @@ void release(nb_extract_batch_t* h) {
     if (h->d_counter) cudaFree(h->d_counter);
     for (auto& job : h->pair_jobs)
         cudaFree(job.second);
+    if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
+    for (cudaStream_t st : h->side)
+        if (st) cudaStreamDestroy(st);
+    if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+    for (cudaEvent_t e : h->ev_join)
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : h->ev_pairs)
+        if (e) cudaEventDestroy(e);
     delete h;
 }
 
@@ -693,8 +808,13 @@ int nb_extract_batch_create(int32_t remap, const nb_extract_request* requests, i
         h->host_reqs[static_cast<size_t>(i)].a = a;
         h->host_reqs[static_cast<size_t>(i)].pairs = nullptr;
     }
-    plan_pairs(h);
-    h->d_reqs = static_cast<BatchReq*>(device_alloc(h->host_reqs.size() * sizeof(BatchReq)));
+    h->n_requests = n_requests;
+    plan_pairs(h, !(flags & NB_BATCH_PERSISTENT_ONLY));
+    if (const cudaError_t berr = make_branches(h); berr != cudaSuccess) {
+        release(h);
+        return finish_launch(berr);
+    }
+    h->d_reqs = static_cast<BatchReq*>(device_alloc(std::max<size_t>(1, h->host_reqs.size()) * sizeof(BatchReq)));
     h->d_counter = static_cast<unsigned long long*>(h->d_reqs ? device_alloc(sizeof(unsigned long long)) : nullptr);
     if (!h->d_reqs || !h->d_counter) {
         release(h);
@@ -757,8 +877,9 @@ int nb_extract_batch_create(int32_t remap, const nb_extract_request* requests, i
             if (err == cudaSuccess && lerr != cudaSuccess)
                 err = lerr;
         }
+        // Node priorities: the copies' branch was captured from a higher-priority stream.
         if (err == cudaSuccess)
-            err = cudaGraphInstantiate(&h->exec, h->graph, 0);
+            err = cudaGraphInstantiateWithFlags(&h->exec, h->graph, cudaGraphInstantiateFlagUseNodePriority);
         cudaStreamDestroy(cap);
     }
     if (err != cudaSuccess) {
@@ -779,7 +900,7 @@ int nb_extract_batch_info(nb_extract_batch batch, nb_batch_info* info) {
     if (!batch || !info)
         return report_error(NB_ERROR_INVALID, "invalid batch handle");
     const Variant vt = VARIANTS[batch->cfg.variant];
-    info->n_requests = static_cast<int64_t>(batch->host_reqs.size());
+    info->n_requests = batch->n_requests;
     info->n_items = batch->n_items;
     info->tile_h = vt.ty;
     info->tile_w = vt.tx;
@@ -788,6 +909,7 @@ int nb_extract_batch_info(nb_extract_batch batch, nb_batch_info* info) {
     info->tuned_ms = batch->tuned_ms;
     info->from_cache = batch->from_cache;
     info->min_ctas = vt.min_ctas;
+    info->n_direct = static_cast<int32_t>(batch->direct.size());
     return NB_OK;
 }
 
@@ -798,6 +920,11 @@ int nb_extract_batch_destroy(nb_extract_batch batch) {
 
 int nb_extract_batch_launch(int32_t remap, const nb_extract_request_ex* requests, int64_t n_requests,
                             const nb_options* options, void* stream) {
+    return nb_extract_batch_launch_ex(remap, requests, n_requests, options, 0, stream);
+}
+
+int nb_extract_batch_launch_ex(int32_t remap, const nb_extract_request_ex* requests, int64_t n_requests,
+                               const nb_options* options, int32_t flags, void* stream) {
     if (!requests || n_requests <= 0)
         return report_error(NB_ERROR_INVALID, "a batch needs at least one request");
     if (n_requests > (int64_t(1) << 30))
@@ -829,6 +956,24 @@ int nb_extract_batch_launch(int32_t remap, const nb_extract_request_ex* requests
                 return st;
             r.pairs = static_cast<const float4*>(requests[i].volume_pairs);
         }
+    }
+    // Validated: from here on, requests large enough over a pair copy are launched as grids of their
+    // own, in order, and leave the persistent launch.
+    if (!(flags & NB_BATCH_PERSISTENT_ONLY)) {
+        std::vector<BatchReq> keep;
+        for (const BatchReq& r : h.host_reqs) {
+            if (r.pairs &&
+                r.a.n_slices * r.a.slice_h * static_cast<int64_t>(r.a.slice_w / 2 + 1) >= ONESHOT_DIRECT_MIN_PIXELS) {
+                const cudaError_t err = launch_extract_pairs(r.a, r.pairs, s);
+                if (err != cudaSuccess)
+                    return finish_launch(err);
+            } else {
+                keep.push_back(r);
+            }
+        }
+        h.host_reqs.swap(keep);
+        if (h.host_reqs.empty())
+            return finish_launch(cudaSuccess);
     }
     bool all_pairs = true;
     for (const BatchReq& r : h.host_reqs)

@@ -45,15 +45,18 @@ __device__ __forceinline__ float w_value(const ProjArgs& a, const float* table, 
     return w < W_TABLE ? table[w] : windowed_sinc(off, a.efs, a.efb);
 }
 
+// Idx: the type of the linear voxel index, 32-bit when the volume has fewer than 2^31 voxels (its
+// divisions then cost a fifth of the 64-bit ones, which bounded the copy).
+template<typename Idx>
 __global__ void make_pairs(const __grid_constant__ ProjArgs a, float4* __restrict__ pairs) {
     const int D = a.vol_d, H = a.vol_h, WP = a.vol_w / 2 + 1;
-    const int64_t n = static_cast<int64_t>(D) * H * WP;
+    const Idx n = static_cast<Idx>(D) * H * WP;
     const float2* vol = static_cast<const float2*>(a.in.data);
-    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
-         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        const int x = static_cast<int>(i % WP);
-        const int64_t zy = i / WP;
-        const int y = static_cast<int>(zy % H), z = static_cast<int>(zy / H);
+    for (Idx i = blockIdx.x * static_cast<Idx>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<Idx>(gridDim.x) * blockDim.x) {
+        const int x = static_cast<int>(i % static_cast<Idx>(WP));
+        const Idx zy = i / static_cast<Idx>(WP);
+        const int y = static_cast<int>(zy % static_cast<Idx>(H)), z = static_cast<int>(zy / static_cast<Idx>(H));
         const int64_t off = z * a.in.s0 + y * a.in.s1 + x * a.in.s2;
         const float2 v0 = vol[off];
         const float2 v1 = x + 1 < WP ? vol[off + a.in.s2] : make_float2(0.f, 0.f);
@@ -178,20 +181,7 @@ cudaError_t launch_pairs(const ProjArgs& a, cudaStream_t stream, bool& done) {
     if (!pairs)
         return cudaSuccess; // no scratch: the caller takes the generic path
     launch_make_pairs(a, pairs, stream);
-    const int wp = a.slice_w / 2 + 1;
-    const int ntx = (wp + TX - 1) / TX, nty = (a.slice_h + TY * PAIR_PPT - 1) / (TY * PAIR_PPT);
-    const dim3 grid(static_cast<unsigned>(ntx * nty), static_cast<unsigned>(a.n_slices < 65535 ? a.n_slices : 65535));
-    if (a.wsize > 1) {
-        if (a.out_cplx)
-            extract_pairs_w_kernel<true><<<grid, EXTRACT_THREADS, 0, stream>>>(a, pairs, ntx);
-        else
-            extract_pairs_w_kernel<false><<<grid, EXTRACT_THREADS, 0, stream>>>(a, pairs, ntx);
-    } else if (a.out_cplx) {
-        extract_pairs_kernel<true><<<grid, EXTRACT_THREADS, 0, stream>>>(a, pairs, ntx);
-    } else {
-        extract_pairs_kernel<false><<<grid, EXTRACT_THREADS, 0, stream>>>(a, pairs, ntx);
-    }
-    const cudaError_t err = cudaGetLastError();
+    const cudaError_t err = launch_extract_pairs(a, pairs, stream);
     scratch_free(pairs, stream);
     done = err == cudaSuccess;
     return err;
@@ -278,14 +268,46 @@ cudaError_t launch_interp(const ProjArgs& a, cudaStream_t stream) {
 
 } // namespace
 
-cudaError_t launch_make_pairs(const ProjArgs& a, float4* pairs, cudaStream_t stream) {
+cudaError_t launch_extract_pairs(const ProjArgs& a, const float4* pairs, cudaStream_t stream) {
+    if (a.n_slices <= 0)
+        return cudaSuccess;
+    const int wp = a.slice_w / 2 + 1;
+    const int ntx = (wp + TX - 1) / TX, nty = (a.slice_h + TY * PAIR_PPT - 1) / (TY * PAIR_PPT);
+    const dim3 grid(static_cast<unsigned>(ntx * nty), static_cast<unsigned>(a.n_slices < 65535 ? a.n_slices : 65535));
+    if (a.wsize > 1) {
+        if (a.out_cplx)
+            extract_pairs_w_kernel<true><<<grid, EXTRACT_THREADS, 0, stream>>>(a, pairs, ntx);
+        else
+            extract_pairs_w_kernel<false><<<grid, EXTRACT_THREADS, 0, stream>>>(a, pairs, ntx);
+    } else if (a.out_cplx) {
+        extract_pairs_kernel<true><<<grid, EXTRACT_THREADS, 0, stream>>>(a, pairs, ntx);
+    } else {
+        extract_pairs_kernel<false><<<grid, EXTRACT_THREADS, 0, stream>>>(a, pairs, ntx);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_make_pairs(const ProjArgs& a, float4* pairs, cudaStream_t stream, const int* priority) {
     const int64_t vox = static_cast<int64_t>(a.vol_d) * a.vol_h * (a.vol_w / 2 + 1);
     const int threads = 256;
     const int64_t blocks = (vox + threads - 1) / threads;
     const int grid = static_cast<int>(blocks < static_cast<int64_t>(sm_count()) * 16 ? blocks : sm_count() * 16);
-    if (grid > 0)
-        make_pairs<<<grid, threads, 0, stream>>>(a, pairs);
-    return cudaGetLastError();
+    if (grid <= 0)
+        return cudaSuccess;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(static_cast<unsigned>(grid));
+    cfg.blockDim = dim3(threads);
+    cfg.stream = stream;
+    cudaLaunchAttribute attr{};
+    if (priority) {
+        attr.id = cudaLaunchAttributePriority;
+        attr.val.priority = *priority;
+        cfg.attrs = &attr;
+        cfg.numAttrs = 1;
+    }
+    if (vox < (int64_t(1) << 31))
+        return cudaLaunchKernelEx(&cfg, make_pairs<uint32_t>, a, pairs);
+    return cudaLaunchKernelEx(&cfg, make_pairs<int64_t>, a, pairs);
 }
 
 cudaError_t launch_extract(const ProjArgs& a, cudaStream_t stream) {

@@ -109,7 +109,12 @@ inline bool pairs_apply(const ProjArgs& a) {
            vox < (int64_t(1) << 31);
 }
 
-// Writes the pair copy of a.in (a.vol_d x a.vol_h x a.vol_w/2+1 complex values) to `pairs`.
-cudaError_t launch_make_pairs(const ProjArgs& a, float4* pairs, cudaStream_t stream);
+// Writes the pair copy of a.in (a.vol_d x a.vol_h x a.vol_w/2+1 complex values) to `pairs`. With
+// `priority`, the launch carries that scheduling priority (kept by a graph captured from it).
+cudaError_t launch_make_pairs(const ProjArgs& a, float4* pairs, cudaStream_t stream, const int* priority = nullptr);
+
+// The per-call LINEAR extraction over a pair copy of a.in: one grid of (slice tile, slice) CTAs
+// (extract_pairs_kernel, or extract_pairs_w_kernel with a w-window).
+cudaError_t launch_extract_pairs(const ProjArgs& a, const float4* pairs, cudaStream_t stream);
 
 } // namespace nb

@@ -8,9 +8,10 @@ their slices). ``ProjectionServer.poll()`` runs one scheduling round:
 2. admission — waiting requests are admitted in arrival order while their device footprint (outputs,
    accumulators, staged orientations, the insertion's transient accumulator) fits in what the budget
    leaves after the resident volumes; a request larger than the whole budget is rejected;
-3. launches — admitted extractions are packed, up to ``max_batch_slices`` slices, into ONE persistent
-   launch (``nb_extract_batch_launch``: a device work queue over all of them, each volume read through
-   its resident pair copy) on the extraction stream, with at most ``max_inflight_batches`` batches
+3. launches — admitted extractions are packed, up to ``max_batch_slices`` slices, into ONE batched
+   launch (``nb_extract_batch_launch``: each volume read through its resident pair copy, requests of
+   2^21 output pixels or more as grids of their own, the rest through one device work queue) on the
+   extraction stream, with at most ``max_inflight_batches`` batches
    queued there; the insertions admitted in the round are packed the same way into ONE batched
    rasterization (``nb_rasterize_batch_launch``: one scatter and one finalize launch, each request into
    its own zeroed value + weight grids) on one of the insertion streams, round robin.

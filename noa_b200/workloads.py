@@ -36,9 +36,9 @@ def batched(args) -> dict:
     """12,000 extractions (LANCZOS8 by default) over 12 resident volumes (3 each of 128, 192, 256, 384;
     hc2h, cutoff 0.5), in `requests` requests (default 12, one per volume; request i reads volume
     i mod 12) whose slice counts are lognormal (median 1000, sigma 0.5, seeded) rescaled to 12,000.
-    Legs: every request through the per-call API, the captured persistent launch (ExtractBatch) and,
-    for LINEAR, one launch over resident pair copies of the volumes (extract_batch_launch), the form
-    the serving loop uses."""
+    Legs: every request through the per-call API, the captured batch graph (ExtractBatch) and, for
+    LINEAR, the same graph with every request in the persistent kernel (persistent_only) and one launch
+    over resident pair copies of the volumes (extract_batch_launch), the form the serving loop uses."""
     import torch
     from . import fourier_project as fp
     from . import synthetic
@@ -76,8 +76,17 @@ def batched(args) -> dict:
     t_call = _timer(per_call, args.steps, flush)
     t_batch = _timer(batch.run, args.steps, flush)
     total = int(counts.sum())
-    resident = None
+    resident = persistent = None
     if args.interp == "linear":
+        # the same batch with every request in the persistent kernel (no direct grids)
+        pbatch = ExtractBatch("hc2h", reqs, interp=args.interp, autotune=not args.no_autotune, persistent_only=True)
+        for _ in range(args.warmup):
+            pbatch.run()
+        torch.cuda.synchronize()
+        t_pers = _timer(pbatch.run, args.steps, flush)
+        persistent = {"ms": statistics.median(t_pers),
+                      "speedup_vs_per_call": statistics.median(t_call) / statistics.median(t_pers)}
+        pbatch.close()
         pairs_v = [volume_pairs(v, (1, n, n, n)) for v, n in zip(vols, boxes)]
         pairs = [pairs_v[i % len(boxes)] for i in range(len(reqs))]
 
@@ -96,6 +105,7 @@ def batched(args) -> dict:
                    "slices_per_volume" if len(reqs) == len(boxes) else "slices_per_request": [int(c) for c in counts],
                    "interp": args.interp, "remap": "hc2h", "cutoff": 0.5, "l2": "flushed before each repetition"},
         "resident_pairs_launch": resident,
+        "persistent_only_graph": persistent,
         "unit": "slices/s",
         "batched": {"value": total / (statistics.median(t_batch) * 1e-3), "ms": statistics.median(t_batch),
                     "launch": batch.info()},

@@ -119,12 +119,43 @@ def test_batch_long_claims_match_per_call(interp, tmp_path, monkeypatch):
     monkeypatch.setenv("NB_AUTOTUNE_CACHE", str(tmp_path / "autotune.txt"))
     # LINEAR batches read pair copies, whose items are 64 x 16 pixels: 4x the slices for as many claims
     reqs, _ = _large_requests([(n, 4 * c) for n, c in LARGE] if interp == "linear" else LARGE)
-    batch = ExtractBatch("hc2h", reqs, interp=interp, autotune=False)
+    batch = ExtractBatch("hc2h", reqs, interp=interp, autotune=False, persistent_only=True)
     info = batch.info()
-    assert info["n_items"] // (info["grid"] * 64) >= 2, info
+    assert info["n_items"] // (info["grid"] * 64) >= 2 and info["n_direct"] == 0, info
     batch.run()
     torch.cuda.synchronize()
     _per_call_equal(reqs, interp)
+    batch.close()
+
+
+def test_batch_direct_grids_match_per_call(tmp_path, monkeypatch):
+    """A LINEAR batch whose large requests run as grids of their own on graph branches (while the
+    other volumes' pair copies are made) and whose small ones go through the persistent kernel: both
+    bit-identical to the per-call entry point, over two replays."""
+    import torch
+    from noa_b200.batch import ExtractBatch
+    monkeypatch.setenv("NB_AUTOTUNE_CACHE", str(tmp_path / "autotune.txt"))
+    # 2^16 output pixels: 32 slices of 64 x 33 reach it, 20 do not; the 112^3 volume is read by too
+    # few pixels for a pair copy (generic LINEAR path, in the persistent kernel)
+    spec = [(128, 1009), (64, 3980), (64, 20), (64, 32), (112, 5), (128, 300)]
+    reqs, _ = _large_requests(spec, seed=9)
+    batch = ExtractBatch("hc2h", reqs, interp="linear", autotune=True)
+    info = batch.info()
+    assert info["n_direct"] == 4 and info["n_requests"] == len(spec) and info["n_items"] > 0, info
+    for _ in range(2):
+        for r in reqs:
+            r.slice.fill_(7)
+        batch.run()
+        torch.cuda.synchronize()
+        _per_call_equal(reqs, "linear")
+    batch.close()
+    # every request direct: no persistent kernel in the graph
+    reqs, _ = _large_requests([(128, 1009), (128, 1100)], seed=10)
+    batch = ExtractBatch("hc2h", reqs, interp="linear", autotune=False)
+    assert batch.info()["n_direct"] == 2 and batch.info()["n_items"] == 0
+    batch.run()
+    torch.cuda.synchronize()
+    _per_call_equal(reqs, "linear")
     batch.close()
 
 
@@ -134,6 +165,12 @@ def test_resident_pairs_long_claims_match_per_call():
     # pair-copy items are 64 x 16 pixels: more slices for the same number of claims
     reqs, vols = _large_requests([(n, 4 * c) for n, c in LARGE], seed=5)
     pairs = {n: volume_pairs(v, (1, n, n, n)) for n, v in vols.items()}
+    extract_batch_launch("hc2h", reqs, [pairs[r.slice_shape[2]] for r in reqs], persistent_only=True)
+    torch.cuda.synchronize()
+    _per_call_equal(reqs, "linear")
+    # the same requests, those of at least 2^21 output pixels as grids of their own
+    for r in reqs:
+        r.slice.fill_(7)
     extract_batch_launch("hc2h", reqs, [pairs[r.slice_shape[2]] for r in reqs])
     torch.cuda.synchronize()
     _per_call_equal(reqs, "linear")
