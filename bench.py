@@ -214,6 +214,9 @@ def run_gpu(args) -> None:
     # slices to insert, rotations) from pinned memory, both calls, D2H of the results. The step is cut
     # into E2E_CHUNKS slice chunks on three streams (copies in, compute, copies out), so the PCIe
     # transfers of both directions overlap each other and the kernels, as a streaming caller would.
+    # (Issuing every extraction chunk first, so that their results stream out from the start, was
+    # slower: 27.1 against 25.6 ms. Both directions at once run at ~47 GB/s each against 55-57 GB/s
+    # alone, so the step is bound by its busier direction at the bidirectional rate, see pcie_gbs.)
     h_vol = vol.cpu().pin_memory()
     h_slices = slices_in.cpu().pin_memory()
     h_rot_e, h_rot_i = rot_e.cpu().pin_memory(), rot_i.cpu().pin_memory()
@@ -272,6 +275,7 @@ def run_gpu(args) -> None:
     e2e = statistics.mean(e2e_ms)
     if world > 1:
         e2e = shard.max_over_ranks([e2e], device="cuda")[0]
+    pcie = pcie_bandwidth(h_slices, slices_in, h_out, out, s_in, s_out)
 
     if rank == 0:
         ab = algorithmic_bytes(N, SLICES)
@@ -311,7 +315,11 @@ def run_gpu(args) -> None:
                                      "extract": "L1 data pipe of the tap gathers"}[dom]},
             "e2e": {"value": total_slices / (e2e * 1e-3), "unit": "slices/s", "h2d_bytes_per_step": bi,
                     "d2h_bytes_per_step": bo, "ms_per_step": e2e,
-                    "schedule": f"{E2E_CHUNKS} slice chunks; copies in, kernels and copies out on 3 streams"},
+                    "schedule": f"{E2E_CHUNKS} slice chunks; copies in, kernels and copies out on 3 streams",
+                    # the same pinned buffers copied alone and both directions at once: the e2e step moves
+                    # max(Bi, Bo) bytes in its busier direction, so that / the bidirectional rate bounds it
+                    "pcie_gbs": pcie,
+                    "pcie_bound_ms": max(bi, bo) / (pcie["both_per_direction"] * 1e9) * 1e3},
             # per step: extract = pair copy + extraction kernel; rasterize = scatter kernel + finalize
             "gpu_launches": 4 * args.steps,
             "clocks": clocks.summary(),
@@ -323,6 +331,49 @@ def run_gpu(args) -> None:
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def pcie_bandwidth(h_a, d_a, h_b, d_b, s_in, s_out, reps: int = 3) -> dict:
+    """Pinned host<->device copy rates (GB/s) of the e2e buffers: h_a -> d_a alone, d_b -> h_b alone,
+    and both at once on two streams (per direction: the smaller of the two bytes / elapsed)."""
+    import torch
+
+    def timed(fn, streams):
+        best = 0.0
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            t0 = torch.cuda.Event(enable_timing=True)
+            t0.record()
+            done = []
+            for s in streams:
+                s.wait_event(t0)
+            fn()
+            for s in streams:
+                e = torch.cuda.Event(enable_timing=True)
+                e.record(s)
+                done.append(e)
+            torch.cuda.synchronize()
+            best = max(best, 1.0 / max(t0.elapsed_time(e) for e in done))
+        return best  # 1 / ms
+
+    na = h_a.numel() * h_a.element_size()
+    nb = h_b.numel() * h_b.element_size()
+
+    def h2d():
+        with torch.cuda.stream(s_in):
+            d_a.copy_(h_a, non_blocking=True)
+
+    def d2h():
+        with torch.cuda.stream(s_out):
+            h_b.copy_(d_b, non_blocking=True)
+
+    def both():
+        h2d()
+        d2h()
+
+    return {"h2d": na * timed(h2d, [s_in]) * 1e3 / 1e9, "d2h": nb * timed(d2h, [s_out]) * 1e3 / 1e9,
+            "both_per_direction": min(na, nb) * timed(both, [s_in, s_out]) * 1e3 / 1e9,
+            "bytes": [na, nb]}
 
 
 # ---------------------------------------------------------------------------------------------------
