@@ -64,7 +64,9 @@ NB_API int nb_extract_batch_create(int32_t remap, const nb_extract_request* requ
                                    const nb_options* options, int32_t flags, void* stream,
                                    nb_extract_batch* batch);
 
-/* Replays the batch on `stream` (asynchronous). Calls on one batch must not overlap on the GPU. */
+/* Replays the batch on `stream` (asynchronous). Calls on one batch must not overlap on the GPU. While
+ * `stream` is being captured into a caller's graph, the batch's launch sequence is issued into that
+ * capture. (nb_extract_batch_create itself synchronizes: inside a capture it returns NB_ERROR_INVALID.) */
 NB_API int nb_extract_batch_run(nb_extract_batch batch, void* stream);
 
 NB_API int nb_extract_batch_info(nb_extract_batch batch, nb_batch_info* info);

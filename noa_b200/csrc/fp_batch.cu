@@ -753,9 +753,8 @@ int launch_once(nb_extract_batch_t& h, KernelFn fn, int variant, int blocks_per_
         return report_error(NB_ERROR_OOM, "cannot allocate the batch descriptors");
     auto* d_reqs = static_cast<BatchReq*>(dev);
     auto* d_counter = reinterpret_cast<unsigned long long*>(static_cast<char*>(dev) + desc_bytes);
-    // Pageable source: the runtime stages it before returning, so the host vector may go right after.
-    cudaError_t err = cudaMemcpyAsync(d_reqs, h.host_reqs.data(), h.host_reqs.size() * sizeof(BatchReq),
-                                      cudaMemcpyHostToDevice, s);
+    // The host vector goes when this returns: upload_async copies it in a form a capture keeps.
+    cudaError_t err = upload_async(d_reqs, h.host_reqs.data(), h.host_reqs.size() * sizeof(BatchReq), s);
     if (err == cudaSuccess)
         err = cudaMemsetAsync(d_counter, 0, sizeof(unsigned long long), s);
     if (err == cudaSuccess) {
@@ -781,6 +780,9 @@ int nb_extract_batch_create(int32_t remap, const nb_extract_request* requests, i
     if (n_requests > (int64_t(1) << 30))
         return report_error(NB_ERROR_INVALID, "too many requests");
     const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (stream_capturing(s))
+        return report_error(NB_ERROR_INVALID, "a batch is created outside a stream capture (creation uploads, "
+                                              "may autotune and synchronizes); its runs may be captured");
     auto* h = new nb_extract_batch_t();
     cudaGetDevice(&h->device);
     h->host_reqs.resize(static_cast<size_t>(n_requests));
@@ -893,7 +895,12 @@ int nb_extract_batch_create(int32_t remap, const nb_extract_request* requests, i
 int nb_extract_batch_run(nb_extract_batch batch, void* stream) {
     if (!batch || !batch->exec)
         return report_error(NB_ERROR_INVALID, "invalid batch handle");
-    return finish_launch(cudaGraphLaunch(batch->exec, static_cast<cudaStream_t>(stream)));
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // Inside a caller's stream capture the batch's launch sequence (the same copies, kernels and
+    // branches its own graph holds) is issued into that capture instead of launching the graph.
+    if (stream_capturing(s))
+        return finish_launch(launch(batch, batch->cfg, s));
+    return finish_launch(cudaGraphLaunch(batch->exec, s));
 }
 
 int nb_extract_batch_info(nb_extract_batch batch, nb_batch_info* info) {

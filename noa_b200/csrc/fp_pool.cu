@@ -2,6 +2,8 @@
 
 #include <atomic>
 #include <cstdint>
+#include <cstring>
+#include <memory>
 #include <mutex>
 
 namespace nb {
@@ -25,7 +27,48 @@ bool within_cap(int dev, size_t bytes) {
     const int64_t c = g_cap_plus1[dev].load(std::memory_order_relaxed);
     return c == 0 || bytes <= static_cast<uint64_t>(c - 1);
 }
+
+// One kernel parameter block of upload_async: 7,500 words (30,000 bytes, under the 32,764-byte
+// parameter limit with the other two arguments).
+constexpr int UPLOAD_WORDS = 7500;
+struct UploadChunk { unsigned w[UPLOAD_WORDS]; };
+
+__global__ void upload_chunk_kernel(const __grid_constant__ UploadChunk c, unsigned* __restrict__ dst, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        dst[i] = c.w[i];
+}
 } // namespace
+
+bool stream_capturing(cudaStream_t stream) {
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(stream, &st) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return st == cudaStreamCaptureStatusActive;
+}
+
+cudaError_t upload_async(void* dst, const void* src, size_t bytes, cudaStream_t stream) {
+    if (bytes == 0)
+        return cudaSuccess;
+    if (bytes % 4 != 0)
+        return cudaErrorInvalidValue;
+    if (!stream_capturing(stream))
+        return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream);
+    const size_t words = bytes / 4;
+    std::unique_ptr<UploadChunk> chunk(new UploadChunk);
+    const unsigned* in = static_cast<const unsigned*>(src);
+    unsigned* out = static_cast<unsigned*>(dst);
+    for (size_t first = 0; first < words; first += UPLOAD_WORDS) {
+        const int n = static_cast<int>(words - first < static_cast<size_t>(UPLOAD_WORDS) ? words - first : UPLOAD_WORDS);
+        std::memcpy(chunk->w, in + first, static_cast<size_t>(n) * 4);
+        upload_chunk_kernel<<<(n + 255) / 256, 256, 0, stream>>>(*chunk, out + first, n);
+        const cudaError_t err = cudaGetLastError();
+        if (err != cudaSuccess)
+            return err;
+    }
+    return cudaSuccess;
+}
 
 bool set_scratch_limit(int device, int64_t bytes) {
     if (device < 0 || device >= MAX_DEVICES)

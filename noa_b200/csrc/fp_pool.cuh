@@ -26,4 +26,14 @@ void* device_alloc(size_t bytes);
 bool set_scratch_limit(int device, int64_t bytes);
 int64_t scratch_limit(int device);
 
+// Copies `bytes` (a multiple of 4) of host memory to device memory in stream order, in a form a
+// stream capture records safely: while `stream` is capturing, the bytes travel as the parameters of
+// small copy kernels (a graph keeps its own copy of every launch's parameters), so replays never read
+// the host buffer; otherwise by cudaMemcpyAsync (the runtime stages pageable memory before
+// returning). Either way the host buffer may be released as soon as this returns.
+cudaError_t upload_async(void* dst, const void* src, size_t bytes, cudaStream_t stream);
+
+// Whether `stream` is being captured into a graph (false if the query fails).
+bool stream_capturing(cudaStream_t stream);
+
 } // namespace nb

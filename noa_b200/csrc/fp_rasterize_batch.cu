@@ -214,7 +214,8 @@ extern "C" int nb_rasterize_batch_launch(int32_t remap, const nb_rasterize_reque
     for (size_t i = 0; i < reqs.size(); ++i)
         reqs[i].acc = scratch + desc_bytes + acc_off[i];
     auto* d_reqs = reinterpret_cast<RasterReq*>(scratch);
-    cudaError_t err = cudaMemcpyAsync(d_reqs, reqs.data(), reqs.size() * sizeof(RasterReq), cudaMemcpyHostToDevice, s);
+    // The host vector goes when this returns: upload_async copies it in a form a capture keeps.
+    cudaError_t err = upload_async(d_reqs, reqs.data(), reqs.size() * sizeof(RasterReq), s);
     if (err == cudaSuccess)
         err = cudaMemsetAsync(scratch + desc_bytes, 0, acc_bytes, s);
     if (err == cudaSuccess) {
