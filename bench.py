@@ -188,6 +188,7 @@ def run_gpu(args) -> None:
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
+    refusals0 = fp.scratch_refusals()
     with ClockSampler(local) as clocks:
         for k in range(args.steps):
             flush.fill_(float(k))          # L2 flush between timed steps (outside the events)
@@ -200,6 +201,7 @@ def run_gpu(args) -> None:
         torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
+    refusals = fp.scratch_refusals() - refusals0
     t_ext = [a.elapsed_time(b) for a, b, _ in ev]
     t_ras = [b.elapsed_time(c) for _, b, c in ev]
     step_ms = sum(t_ext + t_ras) / args.steps
@@ -322,6 +324,8 @@ def run_gpu(args) -> None:
                     "pcie_bound_ms": max(bi, bo) / (pcie["both_per_direction"] * 1e9) * 1e3},
             # per step: extract = pair copy + extraction kernel; rasterize = scatter kernel + finalize
             "gpu_launches": 4 * args.steps,
+            # the library's own allocations refused during the timed steps (each a call on a slower path)
+            "scratch_refusals": refusals,
             "clocks": clocks.summary(),
         }
         if not args.no_secondary and world == 1:
@@ -378,8 +382,8 @@ def pcie_bandwidth(h_a, d_a, h_b, d_b, s_in, s_out, reps: int = 3) -> dict:
 
 # ---------------------------------------------------------------------------------------------------
 # Secondary workloads of the default line, bounded to well under a minute: the small per-call case
-# (64^3), the batched uneven LANCZOS8 extraction against its per-call form in the same run, and the
-# 512^3 windowed-sinc insertion on a subset of its slices, gather against scatter.
+# (64^3), the batched uneven LANCZOS8 and LINEAR extractions against their per-call forms in the same
+# run, and the 512^3 windowed-sinc insertion on a subset of its slices, gather against scatter.
 # ---------------------------------------------------------------------------------------------------
 def _events_ms(fn, reps: int, warmup: int = 3, flush=None) -> float:
     import torch
@@ -434,6 +438,22 @@ def secondary(args) -> dict:
         "timing": "median of 3, L2 flushed before each"}
     torch.cuda.empty_cache()
 
+    # Batched uneven LINEAR: the same 12,000 extractions as 12 and as 120 requests; in the graph, the
+    # requests over pair copies run as grids of their own on parallel branches.
+    for n_req in (12, 120):
+        wargs = argparse.Namespace(seed=0, total=12000, interp="linear", no_autotune=False, steps=3, warmup=2,
+                                   requests=n_req)
+        r = workloads.batched(wargs)
+        out[f"batched_linear_12000_{n_req}req"] = {
+            "workload": f"12,000 LINEAR extractions (hc2h) over 12 volumes of 128, 192, 256, 384 as {n_req} "
+                        "requests, lognormal slice counts; the captured batch graph vs one call per request, "
+                        "same run (both rebuild the volumes' pair copies every run)",
+            "batched_ms": r["batched"]["ms"], "per_call_ms": r["per_call"]["ms"],
+            "persistent_only_ms": r["persistent_only_graph"]["ms"], "direct_grids": r["batched"]["launch"]["n_direct"],
+            "speedup_batched_vs_per_call": r["speedup_batched_vs_per_call"],
+            "timing": "median of 3, L2 flushed before each"}
+        torch.cuda.empty_cache()
+
     # 512^3 windowed-sinc insertion (half-width 6 voxels), gather vs scatter form, on 1000 of the slices.
     n, k = 512, 1000
     wp = n // 2 + 1
@@ -444,6 +464,7 @@ def secondary(args) -> dict:
     ws = fp.WindowedSinc(-1.0, 6.0 / n)
     grids = {}
     times = {}
+    refused = {}
     for name, fn in (("gather", fp.insert_central_slices_3d), ("scatter", fp.insert_central_slices_3d_scatter)):
         v = torch.zeros((1, n, n, wp), dtype=torch.complex64, device="cuda")
         w = torch.zeros((1, n, n, wp), dtype=torch.float32, device="cuda")
@@ -452,8 +473,10 @@ def secondary(args) -> dict:
             fn("hc2hc", slices, None, (k, 1, n, n), v, w, (1, n, n, n), None, rot, interp="linear",
                windowed_sinc=ws, fftfreq_cutoff=0.5)
 
+        r0 = fp.scratch_refusals()
         call()
         torch.cuda.synchronize()
+        refused[name] = fp.scratch_refusals() - r0
         grids[name] = v.clone()
         times[name] = _events_ms(call, 3, warmup=0)
         del v, w
@@ -466,7 +489,10 @@ def secondary(args) -> dict:
                     f"the 20,000 slices of 512x257 c64 into a 512^3 rfft volume",
         "gather_ms": times["gather"], "scatter_ms": times["scatter"],
         "gather_slices_per_s": k / (times["gather"] * 1e-3), "scatter_slices_per_s": k / (times["scatter"] * 1e-3),
-        "scatter_vs_gather_rel_l2": agree, "timing": "median of 3 accumulating calls"}
+        "scatter_vs_gather_rel_l2": agree,
+        # a refused accumulator sends the scatter call to the gather form (then the agreement is exact)
+        "scatter_first_call_without_its_accumulator": refused["scatter"] > 0,
+        "timing": "median of 3 accumulating calls"}
     out["seconds"] = time.perf_counter() - t_start
     return out
 

@@ -191,6 +191,12 @@ NB_API int nb_set_scratch_limit(int32_t device, int64_t bytes);
 /* The cap set on `device` in bytes, -1 when there is none (or the device does not exist). */
 NB_API int64_t nb_scratch_limit(int32_t device);
 
+/* How many of the library's own allocations on `device` were refused since it loaded (above the cap,
+ * or the device out of memory): each sent a call down its path without that memory (same results,
+ * slower) or, for batch descriptors, to NB_ERROR_OOM. A caller that expects the fast paths reads it
+ * before and after its calls. -1 for a bad device index. No counterpart in noa. */
+NB_API int64_t nb_scratch_refusals(int32_t device);
+
 /* Description of the last error on the calling thread ("" if none). */
 NB_API const char* nb_last_error(void);
 

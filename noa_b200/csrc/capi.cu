@@ -636,6 +636,8 @@ int nb_set_scratch_limit(int32_t device, int64_t bytes) {
 
 int64_t nb_scratch_limit(int32_t device) { return nb::scratch_limit(device); }
 
+int64_t nb_scratch_refusals(int32_t device) { return nb::refused_allocations(device); }
+
 int nb_rasterize_central_slices_3d(
     int32_t remap,
     const nb_array* slice, const nb_array* slice_weight, const int64_t slice_shape[4],

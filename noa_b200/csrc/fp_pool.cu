@@ -13,6 +13,9 @@ std::mutex g_mutex;
 cudaMemPool_t g_pools[MAX_DEVICES] = {};
 // Cap + 1 per device; 0 (the zero-initialised default) means no cap.
 std::atomic<int64_t> g_cap_plus1[MAX_DEVICES];
+// Allocations refused per device (above the cap or out of memory): each one sent a call down its
+// path without that memory.
+std::atomic<int64_t> g_refused[MAX_DEVICES];
 
 int current_device() {
     int dev = 0;
@@ -83,10 +86,20 @@ int64_t scratch_limit(int device) {
     return g_cap_plus1[device].load(std::memory_order_relaxed) - 1;
 }
 
+int64_t refused_allocations(int device) {
+    if (device < 0 || device >= MAX_DEVICES)
+        return -1;
+    return g_refused[device].load(std::memory_order_relaxed);
+}
+
 void* scratch_alloc(size_t bytes, cudaStream_t stream) {
     const int dev = current_device();
-    if (dev < 0 || !within_cap(dev, bytes))
+    if (dev < 0)
         return nullptr;
+    if (!within_cap(dev, bytes)) {
+        g_refused[dev].fetch_add(1, std::memory_order_relaxed);
+        return nullptr;
+    }
     cudaMemPool_t pool;
     {
         std::lock_guard<std::mutex> lock(g_mutex);
@@ -109,6 +122,7 @@ void* scratch_alloc(size_t bytes, cudaStream_t stream) {
     void* p = nullptr;
     if (cudaMallocFromPoolAsync(&p, bytes, pool, stream) != cudaSuccess) {
         cudaGetLastError();
+        g_refused[dev].fetch_add(1, std::memory_order_relaxed);
         return nullptr;
     }
     return p;
@@ -121,11 +135,12 @@ void scratch_free(void* ptr, cudaStream_t stream) {
 
 void* device_alloc(size_t bytes) {
     const int dev = current_device();
-    if (dev < 0 || !within_cap(dev, bytes))
+    if (dev < 0)
         return nullptr;
     void* p = nullptr;
-    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+    if (!within_cap(dev, bytes) || cudaMalloc(&p, bytes) != cudaSuccess) {
         cudaGetLastError();
+        g_refused[dev].fetch_add(1, std::memory_order_relaxed);
         return nullptr;
     }
     return p;

@@ -26,6 +26,10 @@ void* device_alloc(size_t bytes);
 bool set_scratch_limit(int device, int64_t bytes);
 int64_t scratch_limit(int device);
 
+// How many allocations scratch_alloc and device_alloc refused on `device` since the library loaded
+// (-1 for a bad device index).
+int64_t refused_allocations(int device);
+
 // Copies `bytes` (a multiple of 4) of host memory to device memory in stream order, in a form a
 // stream capture records safely: while `stream` is capturing, the bytes travel as the parameters of
 // small copy kernels (a graph keeps its own copy of every launch's parameters), so replays never read

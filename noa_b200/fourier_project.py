@@ -89,6 +89,8 @@ def lib() -> C.CDLL:
         h.nb_options_default.argtypes = [opt]
         h.nb_set_scratch_limit.argtypes = [C.c_int32, C.c_int64]
         h.nb_set_scratch_limit.restype = C.c_int
+        h.nb_scratch_refusals.argtypes = [C.c_int32]
+        h.nb_scratch_refusals.restype = C.c_int64
         h.nb_scratch_limit.argtypes = [C.c_int32]
         h.nb_scratch_limit.restype = C.c_int64
         _lib_handle = h
@@ -374,3 +376,9 @@ def scratch_limit(device=None) -> int | None:
     """The cap set with ``set_scratch_limit`` (None when there is none)."""
     v = int(lib().nb_scratch_limit(_device_index(device)))
     return None if v < 0 else v
+
+
+def scratch_refusals(device=None) -> int:
+    """How many of the library's own allocations on ``device`` were refused since it loaded (above the
+    cap or out of memory), each sending a call down its path without that memory."""
+    return int(lib().nb_scratch_refusals(_device_index(device)))

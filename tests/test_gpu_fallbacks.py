@@ -87,9 +87,12 @@ def test_scatter_insert_without_accumulator_is_the_gather_form(cap):
     call = build(default_case("insert", n=40, nslices=30, out_w=True, sinc=(-1.0, 6 / 40), remap="hc2hc",
                               seed=703))
     ref = _oracle(call)
+    from noa_b200 import fourier_project as fp
     gather, gather_w = gpu_run.run(clone(call))
     cap(0)
+    before = fp.scratch_refusals()
     out, out_w = gpu_run.run(clone(call), scatter=True)
+    assert fp.scratch_refusals() == before + 1  # the refused accumulator is counted
     np.testing.assert_array_equal(out, gather)
     np.testing.assert_array_equal(out_w, gather_w)
     assert rel_l2(out, ref.out) <= 1e-5
