@@ -39,7 +39,7 @@ SLICES = 4096
 BFACTOR = 100.0
 L2_FLUSH_BYTES = 256 << 20      # > 126 MB L2
 REFERENCE_SECONDS = 150.0       # bound on the timed steps of the reference arm
-E2E_CHUNKS = 8                  # slice chunks of the end-to-end step (overlapped copies)
+E2E_CHUNKS = 16                 # slice chunks of the end-to-end step (overlapped copies; 16 vs 8: 26.5-26.9 vs 27.0-28.2 ms)
 
 
 def algorithmic_bytes(n: int, b: int) -> dict:
