@@ -490,7 +490,8 @@ def secondary(args) -> dict:
         "gather_ms": times["gather"], "scatter_ms": times["scatter"],
         "gather_slices_per_s": k / (times["gather"] * 1e-3), "scatter_slices_per_s": k / (times["scatter"] * 1e-3),
         "scatter_vs_gather_rel_l2": agree,
-        # a refused accumulator sends the scatter call to the gather form (then the agreement is exact)
+        # a refused accumulator sends the scatter call to the gather form (the agreement is then exact;
+        # it is also exact, with the accumulator, when every voxel's atomics arrive in slice order)
         "scatter_first_call_without_its_accumulator": refused["scatter"] > 0,
         "timing": "median of 3 accumulating calls"}
     out["seconds"] = time.perf_counter() - t_start
