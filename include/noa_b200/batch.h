@@ -1,9 +1,11 @@
-/* noa_b200 — batched extraction (many extract_central_slices_3d calls in one persistent launch) and
- * batched rasterization (many rasterize_central_slices_3d calls in one launch of each kernel).
+/* noa_b200 — batched extraction (many extract_central_slices_3d calls in one captured graph or one
+ * batched launch) and batched rasterization (many rasterize_central_slices_3d calls in one launch of
+ * each kernel).
  *
  * No single function of the reference corresponds to this: it executes a list of
  * extract_central_slices_3d calls (noa/xform/FourierProject.hpp:1869-1914) — different volumes, box
- * sizes and slice counts — as ONE persistent kernel fed by a device work queue, captured once into a
+ * sizes and slice counts — as ONE persistent kernel fed by a device work queue, except that large
+ * LINEAR requests read through pair copies run as grids of their own beside it; captured once into a
  * CUDA graph and replayed. Every request is validated like nb_extract_central_slices_3d and produces
  * bit-identical results. All requests of a batch share `remap` and `options`; their value types
  * (c32->c32, c32->f32 or f32->f32) must agree; each volume must span fewer than 2^31 elements.

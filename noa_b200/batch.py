@@ -1,7 +1,8 @@
 """Batched extraction and rasterization (Python side of include/noa_b200/batch.h).
 
 ``ExtractBatch`` takes a list of extract_central_slices_3d calls — any mix of volumes, box sizes and
-slice counts — and runs them as one persistent kernel captured in a CUDA graph. Build it once, then
+slice counts — and runs them as one CUDA graph: one persistent work-queue kernel, with large LINEAR
+requests read through pair copies as grids of their own on parallel branches. Build it once, then
 ``run()`` it as often as needed; the tensors it was given must stay alive and unchanged in shape.
 """
 from __future__ import annotations

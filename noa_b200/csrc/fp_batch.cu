@@ -1,5 +1,7 @@
 // Batched extraction: many extract_central_slices_3d calls — different volumes, box sizes and slice
-// counts — executed by ONE persistent kernel, replayed as a CUDA graph.
+// counts — executed by ONE persistent kernel, replayed as a CUDA graph; LINEAR requests read through
+// pair copies with enough pixels run instead as grids of the per-call pair kernel on parallel graph
+// branches (nb_extract_batch_t::direct).
 //
 // Work decomposition: every request is cut into (slice, tile) items, a tile being TY x TX pixels of
 // one output slice (4 TY x TX for a request read through its volume's pair copy, 4 rows per thread).
@@ -15,7 +17,7 @@
 // nb_extract_batch_create validates every request like the per-call entry point, uploads the request
 // descriptors once, optionally autotunes (tile shape x CTAs per SM, timed on the batch itself and
 // cached per workload key in memory and in a small text file), and captures the launch — the pair
-// copies of LINEAR batches, counter reset, persistent kernel — into a CUDA graph.
+// copies of LINEAR batches, the direct grids, counter reset, persistent kernel — into a CUDA graph.
 // nb_extract_batch_run replays that graph on a stream.
 #include "fp_args.cuh"
 #include "fp_pairs.cuh"
