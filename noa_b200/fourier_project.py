@@ -109,10 +109,15 @@ def _torch():
     return torch
 
 
+_DTYPES: dict = {}
+
+
 def _dtype_code(t) -> int:
-    torch = _torch()
-    return {torch.float32: DTYPE_F32, torch.complex64: DTYPE_C32,
-            torch.float64: DTYPE_F64, torch.complex128: DTYPE_C64}[t.dtype]
+    if not _DTYPES:
+        torch = _torch()
+        _DTYPES.update({torch.float32: DTYPE_F32, torch.complex64: DTYPE_C32,
+                        torch.float64: DTYPE_F64, torch.complex128: DTYPE_C64})
+    return _DTYPES[t.dtype]
 
 
 def as_nb_array(t, keep: list) -> NbArray | None:
@@ -126,13 +131,13 @@ def as_nb_array(t, keep: list) -> NbArray | None:
         a.value[0] = float(np.real(t))
         a.value[1] = float(np.imag(t))
         return a
-    if t.dim() != 4:
-        raise NoaB200Error(NB_ERROR_INVALID, f"expected a 4-D (BDHW) tensor, got shape {tuple(t.shape)}")
+    shape = t.shape
+    if len(shape) != 4:
+        raise NoaB200Error(NB_ERROR_INVALID, f"expected a 4-D (BDHW) tensor, got shape {tuple(shape)}")
     a.data = t.data_ptr()
     a.dtype = _dtype_code(t)
-    for i in range(4):
-        a.shape[i] = t.shape[i]
-        a.strides[i] = t.stride(i)
+    a.shape[:] = shape
+    a.strides[:] = t.stride()
     keep.append(t)
     return a
 
@@ -198,21 +203,33 @@ class WindowedSinc:
     fftfreq_blackman: float = -1.0
 
 
+_DEFAULT_OPTIONS: list = []
+_NO_WINDOW = WindowedSinc()
+
+
+def _default_options() -> NbOptions:
+    """The library's default options (nb_options_default), fetched once."""
+    if not _DEFAULT_OPTIONS:
+        o = NbOptions()
+        lib().nb_options_default(C.byref(o))
+        _DEFAULT_OPTIONS.append(o)
+    return _DEFAULT_OPTIONS[0]
+
+
 def _options(interp="linear", fftfreq_cutoff=0.5, target_shape=None, ews_radius=(0.0, 0.0),
              windowed_sinc: WindowedSinc | None = None, w_windowed_sinc: WindowedSinc | None = None,
              add_to_output=False, correct_weights=False) -> NbOptions:
-    o = NbOptions()
-    lib().nb_options_default(C.byref(o))
+    o = NbOptions.from_buffer_copy(_default_options())
     o.interp = INTERPS[interp] if isinstance(interp, str) else int(interp)
     o.fftfreq_cutoff = float(fftfreq_cutoff)
     if target_shape is not None:
         for i in range(4):
             o.target_shape[i] = int(target_shape[i])
-    if np.isscalar(ews_radius):
+    if isinstance(ews_radius, (int, float)) or np.isscalar(ews_radius):
         ews_radius = (ews_radius, ews_radius)
     o.ews_radius[0], o.ews_radius[1] = float(ews_radius[0]), float(ews_radius[1])
-    ws = windowed_sinc or WindowedSinc()
-    wws = w_windowed_sinc or WindowedSinc()
+    ws = windowed_sinc or _NO_WINDOW
+    wws = w_windowed_sinc or _NO_WINDOW
     o.fftfreq_sinc, o.fftfreq_blackman = float(ws.fftfreq_sinc), float(ws.fftfreq_blackman)
     o.w_fftfreq_sinc, o.w_fftfreq_blackman = float(wws.fftfreq_sinc), float(wws.fftfreq_blackman)
     o.add_to_output = int(bool(add_to_output))
@@ -234,8 +251,11 @@ def _check(code: int) -> None:
         raise NoaB200Error(code, lib().nb_last_error().decode(errors="replace"))
 
 
+_I64x4 = C.c_int64 * 4
+
+
 def _shape(s) -> C.Array:
-    return (C.c_int64 * 4)(*[int(v) for v in s])
+    return _I64x4(*map(int, s))
 
 
 def _ref(x):
