@@ -69,3 +69,49 @@ def test_rasterize_into_a_grid_spanning_2_31_elements(big_buffer):
     got = wide.contiguous()
     rel = float(((got - compact).abs().pow(2).sum() / compact.abs().pow(2).sum()).sqrt())
     assert compact.abs().max().item() > 0 and rel <= 1e-6, rel
+
+
+def _wide_slices(buf, count):
+    """count slices of N x (N/2+1) whose rows lie 35 M elements apart (the slices interleaved along x,
+    batch stride N/2+1): offsets within one slice need 64 bits."""
+    import torch
+    wp = N // 2 + 1
+    assert count * wp <= DEPTH_STRIDE
+    return torch.as_strided(buf, (count, 1, N, wp), (wp, wp, DEPTH_STRIDE, 1))
+
+
+def test_insertions_from_slices_spanning_2_31_elements(big_buffer):
+    import torch
+    from noa_b200 import fourier_project as fp
+    from noa_b200 import synthetic
+    count = 24
+    compact = torch.from_numpy(synthetic.make_slices(count, N, seed=35)).cuda()
+    wide = _wide_slices(big_buffer, count)
+    wide.copy_(compact)
+    assert (wide.shape[2] - 1) * wide.stride(2) >= 2 ** 31 - 1
+    rot = torch.from_numpy(synthetic.random_rotations(count, seed=36)).cuda()
+    inv = fp.pack_rotations(rot.transpose(1, 2).contiguous())
+    fwd = fp.pack_rotations(rot)
+    rot_out = fp.pack_rotations(torch.from_numpy(synthetic.random_rotations(5, seed=37)).cuda())
+    ws = fp.WindowedSinc(-1.0, 3.0 / N)
+    res = {}
+    for name, sl in (("wide", wide), ("compact", compact)):
+        g = torch.zeros((1, N, N, N // 2 + 1), dtype=torch.complex64, device="cuda")
+        gs = torch.zeros_like(g)
+        gr = torch.zeros_like(g)
+        o = torch.full((5, 1, N, N // 2 + 1), 7, dtype=torch.complex64, device="cuda")
+        fp.insert_central_slices_3d("h2hc", sl, None, (count, 1, N, N), g, None, (1, N, N, N), None, inv,
+                                    windowed_sinc=ws)
+        fp.insert_central_slices_3d_scatter("h2hc", sl, None, (count, 1, N, N), gs, None, (1, N, N, N), None, inv,
+                                            windowed_sinc=ws)
+        fp.rasterize_central_slices_3d("h2hc", sl, None, (count, 1, N, N), gr, None, (1, N, N, N), None, fwd)
+        fp.insert_and_extract_central_slices_3d("h2h", sl, None, (count, 1, N, N), o, None, (5, 1, N, N), None, inv,
+                                                None, rot_out, input_windowed_sinc=ws)
+        res[name] = (g, gs, gr, o)
+    torch.cuda.synchronize()
+    (g, gs, gr, o), (g2, gs2, gr2, o2) = res["wide"], res["compact"]
+    assert g2.abs().max().item() > 0 and o2.abs().max().item() > 0
+    assert torch.equal(g, g2) and torch.equal(o, o2)  # deterministic gathers: bit for bit
+    for a, b in ((gs, gs2), (gr, gr2)):  # atomic scatters: summation order only
+        rel = float(((a - b).abs().pow(2).sum() / b.abs().pow(2).sum()).sqrt())
+        assert rel <= 1e-6, rel
