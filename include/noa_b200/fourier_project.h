@@ -35,7 +35,7 @@ enum {
     NB_ERROR_UNSUPPORTED = -2,  /* valid for noa but not provided here (f64/c64 values, textures) */
     NB_ERROR_CUDA = -3,         /* a CUDA runtime call failed */
     NB_ERROR_OOM = -4,          /* a scratch or device allocation failed */
-    NB_ERROR_TIMEOUT = -5       /* a bounded device wait ran out (batched/serving paths only) */
+    NB_ERROR_TIMEOUT = -5       /* reserved: no kernel of this library waits on the device, so none returns it */
 };
 
 /* noa::fft::Layout values of the four hx2hx remaps (fft/core/Layout.hpp:48-55). */

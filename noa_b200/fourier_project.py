@@ -23,7 +23,7 @@ NB_ERROR_INVALID = -1
 NB_ERROR_UNSUPPORTED = -2
 NB_ERROR_CUDA = -3
 NB_ERROR_OOM = -4
-NB_ERROR_TIMEOUT = -5
+NB_ERROR_TIMEOUT = -5  # reserved (no kernel waits on the device)
 
 REMAPS = {"h2h": 0, "h2hc": 8, "hc2h": 4, "hc2hc": 12}
 INTERPS = {"nearest": 0, "linear": 1, "cubic": 2, "cubic_bspline": 3, "lanczos4": 4, "lanczos6": 5,
