@@ -17,8 +17,15 @@ namespace {
 constexpr int BZ = 4, BY = 8, BX = 8;
 constexpr int INSERT_THREADS = BZ * BY * BX;
 
+// CTAs per SM the LINEAR and NEAREST instantiations are compiled for (32 registers, small spills): the
+// kernel is issue-bound and more resident warps hide its latencies: 512^3 x 20,000 slices, 328.9 ->
+// 286.2-287.1 ms on one box (1000 slices: 16.13 -> 13.50-13.64 ms; six CTAs 13.80-13.86 ms). The
+// wider windows keep the compiler's choice.
+template<int I>
+constexpr int insert_min_ctas() { return I == I_LINEAR || I == I_NEAREST ? 8 : 1; }
+
 template<int I, bool IN_C, bool OUT_C>
-__global__ void __launch_bounds__(INSERT_THREADS)
+__global__ void __launch_bounds__(INSERT_THREADS, insert_min_ctas<I>())
 insert_kernel(const __grid_constant__ ProjArgs a, int nbz, int nby, int nbx) {
     __shared__ int s_list[INSERT_THREADS];
     __shared__ int s_warp_count[INSERT_THREADS / 32];
